@@ -1,0 +1,112 @@
+// gg_handle.h -- host-side state of one Stokes problem (opaque gg_handle of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gg_internal.cuh"
+
+namespace gg {
+
+// Device scalars of one Krylov solve (written and read by kernels only).
+struct KrylovScalars {
+    double rz, rz_old, pAp, alpha, beta;
+    double rnorm, rnorm0, ttol;
+    double partial_pad[8];
+    int32_t done, iterations, failed, maxit;
+};
+
+// A device buffer with RAII.
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void ensure(size_t nbytes) {
+        if (nbytes <= bytes && p) return;
+        release();
+        size_t b = nbytes ? nbytes : 16;
+        GG_CUDA(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// One multigrid level (level 0 = the fine mesh).
+struct MGLevel {
+    MeshK mk;
+    int64_t nnode = 0, nel = 0;
+    DBuf mom32, mom64, diag32, bcmask;
+    DBuf x, r, b, t;  // FP32 work vectors [dim*nnode]
+    double lambda_max = 0.0;
+};
+
+struct Handle {
+    gg_mesh_desc desc{};
+    MeshK mk{};
+    int dim = 0, nm = 0;
+    int64_t nel = 0, nnode = 0, ndof = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    // mesh-level data
+    DBuf bcmask, bcval, T;
+    bool has_T = false, has_bc = false;
+    int64_t nfree = 0;  // velocity dofs without a Dirichlet condition
+    gg_body_force force{};
+    int n_materials = 0;
+    std::vector<gg_material> materials;
+
+    // points
+    int64_t np = 0, np_in = 0;
+    DBuf coords, mat_in, ps_in, cell, perm, cell_s, xi_s, mat_s, ps_s, eta_s, incr_s, yld_s;
+    DBuf offsets, fill, scan_tmp, flag;
+    bool located = false;
+
+    // operator
+    DBuf mom64, mom32, kdiag64, kdiag32, sdiag, hvec, f;
+    bool built = false;
+    int built_precision = -1;
+    DBuf prev_u, prev_p;  // previous solution read by the yield laws (SoA / element)
+
+    // solver work
+    DBuf u, vstar, ftmp, ub, q, qtmp, r, s;           // FP64
+    DBuf cg_b, cg_r, cg_z, cg_p, cg_Ap, cg_x;        // FP64 CG
+    DBuf r32, cgr32, z32, p32, Ap32, e32;             // FP32 inner CG
+    DBuf scal, red;                                   // KrylovScalars, reduction scratch
+    KrylovScalars* h_scal = nullptr;                  // pinned mirror
+    std::vector<std::unique_ptr<MGLevel>> mg;
+    bool mg_ready = false;
+    DBuf coarse_inv;  // dense inverse of the coarsest operator (FP32)
+    int64_t coarse_n = 0;
+
+    // CUDA graphs keyed by solver variant
+    std::map<std::string, cudaGraphExec_t> graphs;
+    double last_solve_ms = 0.0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    // last solution (for advection and Picard)
+    bool have_solution = false;
+    int32_t max_material = 0;       // largest material index of the points
+    mutable int64_t kernel_launches = 0;    // launches of this library's kernels (graph nodes counted)
+    DBuf picard_prev, picard_part;
+};
+
+}  // namespace gg
+
+// The opaque handle of the C ABI.
+struct gg_handle {
+    gg::Handle H;
+};

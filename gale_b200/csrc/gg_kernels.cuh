@@ -1,0 +1,66 @@
+// gg_kernels.cuh -- declarations shared by the .cu translation units and the inline
+// device helpers of the regular Q1 mesh.
+#pragma once
+
+#include "gg_handle.h"
+#include "gg_internal.cuh"
+
+namespace gg {
+
+int num_sms();
+int grid_for(int64_t n, int block);
+
+// Vertex coordinate, CartesianGenerator_CalcGeom (StgDomain/Mesh/src/
+// CartesianGenerator.cxx:2178-2215), with explicit roundings (no FMA contraction).
+__device__ __forceinline__ double vert_coord_d(const MeshK& mk, int d, int i) {
+    if (i == 0) return mk.min[d];
+    if (i == mk.n[d]) return mk.max[d];
+    return __dadd_rn(mk.min[d], __dmul_rn(__ddiv_rn((double)i, (double)mk.n[d]),
+                                          __dsub_rn(mk.max[d], mk.min[d])));
+}
+
+__device__ __forceinline__ void elem_ijk(const MeshK& mk, int64_t e, int* ijk) {
+    ijk[0] = (int)(e % mk.n[0]);
+    const int64_t r = e / mk.n[0];
+    ijk[1] = (int)(r % mk.n[1]);
+    ijk[2] = (int)(r / mk.n[1]);
+}
+
+template <int DIM>
+__device__ __forceinline__ int64_t elem_node(const MeshK& mk, const int* ijk, int a) {
+    const int i = ijk[0] + (a & 1), j = ijk[1] + ((a >> 1) & 1);
+    const int k = DIM == 3 ? ijk[2] + ((a >> 2) & 1) : 0;
+    return i + (int64_t)mk.nn[0] * (j + (int64_t)mk.nn[1] * k);
+}
+
+// ---- host drivers ------------------------------------------------------------------
+int64_t locate_and_sort(Handle& H);
+
+// Per-point rheology + moments + force + diagonals.  precision GG_PRECISION_FP64 fills
+// mom64/kdiag64/sdiag/f/eta; GG_PRECISION_MIXED additionally fills mom32/kdiag32 with
+// the FP32 rheology and FP32 element sums.  Returns 0 or a GG_ERR code.
+int build_operator(Handle& H, int precision, int prev, const double* d_prev_u,
+                   const double* d_prev_p);
+
+// y = K x on one level (level mesh mk, moments mom, bc mask); y is accumulated with
+// atomics and must be zero on entry; BC rows of y are left untouched (zero).
+// energy (nullable): per-block partials of Σ_e x_eᵀ K_e x_e.
+template <typename R>
+void apply_K(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
+             cudaStream_t st);
+void apply_G(const Handle& H, const double* p, double* y, cudaStream_t st);
+void apply_GT(const Handle& H, const double* u, double* q, cudaStream_t st);
+
+// Krylov / Uzawa (gg_solve.cu)
+int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& st);
+int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* x,
+                double rtol, int maxit, int* iters);
+void release_graphs(Handle& H);
+
+// prev_u = u + BC values, prev_p = q (gg_api2.cu)
+void store_solution(Handle& H);
+
+// Advection (gg_advect.cu)
+int advect(Handle& H, double dt, int order, const double* d_u, double* d_out);
+
+}  // namespace gg

@@ -1,0 +1,154 @@
+// gg_ops.cu -- matrix-free K, G and Gᵀ on sm_100a.
+//
+// K apply (replaces MatMult with the assembled k_matrix of __StiffnessMatrix_NewAssemble,
+// StgFEM/SLE/SystemSetup/src/StiffnessMatrix.cxx:2016-2200).  One thread per element:
+//   1. gather the 2^dim nodal values per component (coalesced along x),
+//   2. Walsh–Hadamard transform → modal coefficients m[c][S] = Σ_a Π_{d∈S} s_d(a) u_a,c,
+//   3. velocity gradient ∂u_c/∂x_d = κ_d Σ_{T⊆others(d)} m[c][{d}∪T] ξ^T,
+//   4. stress σ = 2ε̇ (viscosity is inside the moments), projected on the test basis
+//      through the element moments M[U+T] = Σ_p c_p ξ_p^{U+T},
+//   5. inverse transform → y_e, scattered with atomics (BC rows skipped).
+// The same pass returns x_eᵀ K_e x_e, so Σ_e gives pᵀKp for CG without a second pass.
+// Bandwidth-bound (nodal vectors + n_mom moments per element); no tensor cores.
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+#include "gg_ops.cuh"
+
+namespace gg {
+
+template <int DIM, typename R>
+__global__ void __launch_bounds__(256)
+k_apply_K(MeshK mk, const R* __restrict__ mom, const uint8_t* __restrict__ bcmask,
+          const R* __restrict__ x, R* __restrict__ y, double* __restrict__ energy_part) {
+    constexpr int NS = 1 << DIM;
+    const int64_t nel = mk.nel, nnode = mk.nnode;
+    double en = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int ijk[3];
+        elem_ijk(mk, e, ijk);
+        int64_t nodes[NS];
+        R u[NS][DIM], yl[NS][DIM];
+#pragma unroll
+        for (int a = 0; a < NS; a++) {
+            nodes[a] = elem_node<DIM>(mk, ijk, a);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) u[a][c] = x[(int64_t)c * nnode + nodes[a]];
+        }
+        element_apply_dev<DIM, R>(mk, mom, nel, e, u, yl);
+#pragma unroll
+        for (int a = 0; a < NS; a++) {
+            const uint8_t bm = bcmask[nodes[a]];
+#pragma unroll
+            for (int c = 0; c < DIM; c++) {
+                en += (double)u[a][c] * (double)yl[a][c];
+                if (!((bm >> c) & 1)) atomicAdd(&y[(int64_t)c * nnode + nodes[a]], yl[a][c]);
+            }
+        }
+    }
+    if (energy_part) {
+        en = block_sum(en);
+        if (threadIdx.x == 0) energy_part[blockIdx.x] = en;
+    }
+}
+
+template <typename R>
+void apply_K_ex(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
+                double* energy_part, int grid, cudaStream_t st) {
+    if (mk.dim == 2)
+        k_apply_K<2, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part);
+    else
+        k_apply_K<3, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part);
+}
+template void apply_K_ex<double>(const MeshK&, const double*, const uint8_t*, const double*, double*,
+                                 double*, int, cudaStream_t);
+template void apply_K_ex<float>(const MeshK&, const float*, const uint8_t*, const float*, float*,
+                                double*, int, cudaStream_t);
+
+template <typename R>
+void apply_K(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y, cudaStream_t st) {
+    apply_K_ex<R>(mk, mom, bcmask, x, y, nullptr, apply_grid(mk.nel), st);
+    GG_CUDA(cudaGetLastError());
+}
+template void apply_K<double>(const MeshK&, const double*, const uint8_t*, const double*, double*,
+                              cudaStream_t);
+template void apply_K<float>(const MeshK&, const float*, const uint8_t*, const float*, float*,
+                             cudaStream_t);
+
+int apply_grid(int64_t nel) {
+    int64_t g = (nel + 255) / 256;
+    const int cap = num_sms() * 8;
+    return (int)(g < cap ? (g < 1 ? 1 : g) : cap);
+}
+
+// ---- G p (P0 pressure → velocity force): node-centric gather, BC rows zero ----------
+// G_e[a][c] = Σ_gauss w (−detJ) ∂N_a/∂x_c (GradientStiffnessMatrixTerm.cxx:213-246).
+template <int DIM, typename R>
+__global__ void k_apply_G(MeshK mk, const uint8_t* __restrict__ bcmask, const R* __restrict__ p,
+                          R* __restrict__ y, R beta) {
+    const int64_t nnode = mk.nnode;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nnode;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(n % mk.nn[0]);
+        const int j = (int)((n / mk.nn[0]) % mk.nn[1]);
+        const int k = DIM == 3 ? (int)(n / ((int64_t)mk.nn[0] * mk.nn[1])) : 0;
+        R acc[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) acc[c] = R(0);
+#pragma unroll
+        for (int a = 0; a < (1 << DIM); a++) {
+            const int ei = i - (a & 1), ej = j - ((a >> 1) & 1), ek = DIM == 3 ? k - ((a >> 2) & 1) : 0;
+            if (ei < 0 || ej < 0 || ek < 0 || ei >= mk.n[0] || ej >= mk.n[1] || ek >= mk.n[2]) continue;
+            const R pv = p[ei + (int64_t)mk.n[0] * (ej + (int64_t)mk.n[1] * ek)];
+#pragma unroll
+            for (int c = 0; c < DIM; c++) acc[c] += (R)mk.Ge[a][c] * pv;
+        }
+        const uint8_t bm = bcmask[n];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) {
+            R* yp = &y[(int64_t)c * nnode + n];
+            *yp = ((bm >> c) & 1) ? R(0) : (beta == R(0) ? acc[c] : beta * (*yp) + acc[c]);
+        }
+    }
+}
+
+// ---- Gᵀ u (velocity → element): element-centric, all columns --------------------------
+template <int DIM, typename R>
+__global__ void k_apply_GT(MeshK mk, const R* __restrict__ u, R* __restrict__ q) {
+    const int64_t nel = mk.nel, nnode = mk.nnode;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int ijk[3];
+        elem_ijk(mk, e, ijk);
+        R s = R(0);
+#pragma unroll
+        for (int a = 0; a < (1 << DIM); a++) {
+            const int64_t n = elem_node<DIM>(mk, ijk, a);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) s += (R)mk.Ge[a][c] * u[(int64_t)c * nnode + n];
+        }
+        q[e] = s;
+    }
+}
+
+void apply_G(const Handle& H, const double* p, double* y, cudaStream_t st) {
+    const int g = grid_for(H.nnode, 256);
+    if (H.dim == 2)
+        k_apply_G<2, double><<<g, 256, 0, st>>>(H.mk, H.bcmask.as<uint8_t>(), p, y, 0.0);
+    else
+        k_apply_G<3, double><<<g, 256, 0, st>>>(H.mk, H.bcmask.as<uint8_t>(), p, y, 0.0);
+    GG_CUDA(cudaGetLastError());
+    H.kernel_launches++;
+}
+
+void apply_GT(const Handle& H, const double* u, double* q, cudaStream_t st) {
+    const int g = grid_for(H.nel, 256);
+    if (H.dim == 2)
+        k_apply_GT<2, double><<<g, 256, 0, st>>>(H.mk, u, q);
+    else
+        k_apply_GT<3, double><<<g, 256, 0, st>>>(H.mk, u, q);
+    GG_CUDA(cudaGetLastError());
+    H.kernel_launches++;
+}
+
+}  // namespace gg

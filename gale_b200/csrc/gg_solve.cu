@@ -1,0 +1,535 @@
+// gg_solve.cu -- inner velocity Krylov solves and the Uzawa outer iteration on sm_100a.
+//
+// Inner solve (replaces KSPSolve(velSolver, ...) at Stokes_SLE_UzawaSolver.cxx:554,620,725
+// with PETSc CG + PCJACOBI: zero initial guess, preconditioned residual norm,
+// rnorm ≤ max(rtol·rnorm0, 1e-50)).  One CG iteration is three kernels whose scalars
+// live on the device (last-block reductions in a fixed order), captured as a CUDA graph
+// of kChunk iterations; the host only polls the done flag between graph launches.
+//   k_apply_K      Ap = K p and pᵀKp from the element energies → α (last block)
+//   k_cg_update    x += αp, r −= αAp, z = D⁻¹r, Ap = 0, (z,z), (r,z) → β, convergence
+//   k_cg_direction p = z + βp
+// Mixed precision (GG_PRECISION_MIXED): FP64 defect correction around FP32 CG solves
+// of K32 e = r32 with FP32 moments; the defect r = b − K64 x and the stopping test stay
+// in FP64.
+//
+// Outer solve: _Stokes_SLE_UzawaSolver_Solve (Stokes_SLE_UzawaSolver.cxx:393-938) step
+// for step, with the Ĝ = Gᵀ diag(K_e)⁻¹ G preconditioner (diagonal for P0).
+#include <math.h>
+
+#include <stdio.h>
+
+#include <cstring>
+
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+#include "gg_ops.cuh"
+
+namespace gg {
+
+namespace {
+
+constexpr int kRedBlocks = 592;  // 4 × 148 SMs: reduction grid of the vector kernels
+constexpr int kChunk = 16;       // CG iterations per graph launch
+
+struct RedCounter {
+    unsigned int count;
+};
+
+// Last-block pattern: every block writes its partial(s), the last block to arrive sums
+// all partials in block order (deterministic) and runs `fin`.
+template <int NV, class Fin>
+__device__ __forceinline__ void grid_reduce(double (&v)[NV], double* part, unsigned int* counter,
+                                            Fin fin) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double t = block_sum(v[k]);
+        if (threadIdx.x == 0) part[k * gridDim.x + blockIdx.x] = t;
+    }
+    __shared__ bool last;
+    __threadfence();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double tot[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += part[k * gridDim.x + b];
+        // fixed-order block reduction of the strided partial sums
+        s = block_sum(s);
+        tot[k] = s;
+    }
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        fin(tot);
+    }
+}
+
+template <typename V>
+__global__ void k_cg_init(int64_t n, int dim, int64_t nnode, const uint8_t* __restrict__ bcmask,
+                          const V* __restrict__ b, const V* __restrict__ diag, V* __restrict__ x,
+                          V* __restrict__ r, V* __restrict__ z, V* __restrict__ p, V* __restrict__ Ap,
+                          double rtol, int maxit, KrylovScalars* s, double* part, unsigned int* counter) {
+    double acc[2] = {0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i / nnode);
+        const bool fixed = (bcmask[i - (int64_t)c * nnode] >> c) & 1;
+        const V rv = fixed ? V(0) : b[i];
+        const V zv = fixed ? V(0) : rv / diag[i];
+        x[i] = V(0);
+        r[i] = rv;
+        z[i] = zv;
+        p[i] = zv;
+        Ap[i] = V(0);
+        acc[0] += (double)zv * (double)zv;
+        acc[1] += (double)rv * (double)zv;
+    }
+    grid_reduce<2>(acc, part, counter, [=](double* t) {
+        s->rnorm0 = sqrt(t[0]);
+        s->rnorm = s->rnorm0;
+        double tt = rtol * s->rnorm0;
+        s->ttol = tt < 1e-50 ? 1e-50 : tt;
+        s->rz = t[1];
+        s->iterations = 0;
+        s->failed = 0;
+        s->maxit = maxit;
+        s->done = (s->rnorm0 <= s->ttol) ? 1 : 0;
+    });
+}
+
+// Ap = K p, α = rz / pᵀKp.  Fused copy of k_apply_K with the done test and the α finalise.
+template <int DIM, typename V>
+__global__ void __launch_bounds__(256)
+k_cg_apply(MeshK mk, const V* __restrict__ mom, const uint8_t* __restrict__ bcmask,
+           const V* __restrict__ p, V* __restrict__ Ap, KrylovScalars* s, double* part,
+           unsigned int* counter);
+
+template <typename V>
+__global__ void k_cg_update(int64_t n, int64_t nnode, const uint8_t* __restrict__ bcmask,
+                            const V* __restrict__ diag, V* __restrict__ x, V* __restrict__ r,
+                            V* __restrict__ z, const V* __restrict__ p, V* __restrict__ Ap,
+                            KrylovScalars* s, double* part, unsigned int* counter) {
+    if (s->done) return;
+    const V alpha = (V)s->alpha;
+    double acc[2] = {0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i / nnode);
+        const bool fixed = (bcmask[i - (int64_t)c * nnode] >> c) & 1;
+        const V pv = p[i];
+        const V ap = Ap[i];
+        x[i] += alpha * pv;
+        const V rv = fixed ? V(0) : r[i] - alpha * ap;
+        const V zv = fixed ? V(0) : rv / diag[i];
+        r[i] = rv;
+        z[i] = zv;
+        Ap[i] = V(0);
+        acc[0] += (double)zv * (double)zv;
+        acc[1] += (double)rv * (double)zv;
+    }
+    grid_reduce<2>(acc, part, counter, [=](double* t) {
+        const double rn = sqrt(t[0]);
+        s->rnorm = rn;
+        s->iterations += 1;
+        if (!(rn == rn) || isinf(rn)) {
+            s->failed = 2;
+            s->done = 1;
+        } else if (rn <= s->ttol) {
+            s->done = 1;
+        } else if (s->iterations >= s->maxit) {
+            s->failed = 1;
+            s->done = 1;
+        }
+        s->beta = t[1] / s->rz;
+        s->rz = t[1];
+    });
+}
+
+template <typename V>
+__global__ void k_cg_direction(int64_t n, const V* __restrict__ z, V* __restrict__ p,
+                               const KrylovScalars* s) {
+    if (s->done) return;
+    const V beta = (V)s->beta;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+template <int DIM, typename V>
+__global__ void __launch_bounds__(256)
+k_cg_apply(MeshK mk, const V* __restrict__ mom, const uint8_t* __restrict__ bcmask,
+           const V* __restrict__ p, V* __restrict__ Ap, KrylovScalars* s, double* part,
+           unsigned int* counter) {
+    if (s->done) return;
+    constexpr int NS = 1 << DIM;
+    const int64_t nel = mk.nel, nnode = mk.nnode;
+    double en = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int ijk[3];
+        elem_ijk(mk, e, ijk);
+        int64_t nodes[NS];
+        V u[NS][DIM], yl[NS][DIM];
+#pragma unroll
+        for (int a = 0; a < NS; a++) {
+            nodes[a] = elem_node<DIM>(mk, ijk, a);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) u[a][c] = p[(int64_t)c * nnode + nodes[a]];
+        }
+        element_apply_dev<DIM, V>(mk, mom, nel, e, u, yl);
+#pragma unroll
+        for (int a = 0; a < NS; a++) {
+            const uint8_t bm = bcmask[nodes[a]];
+#pragma unroll
+            for (int c = 0; c < DIM; c++) {
+                en += (double)u[a][c] * (double)yl[a][c];
+                if (!((bm >> c) & 1)) atomicAdd(&Ap[(int64_t)c * nnode + nodes[a]], yl[a][c]);
+            }
+        }
+    }
+    double acc[1] = {en};
+    grid_reduce<1>(acc, part, counter, [=](double* t) {
+        s->pAp = t[0];
+        s->alpha = s->rz / t[0];
+        if (!(t[0] > 0.0) || isinf(t[0])) {
+            s->failed = 3;
+            s->done = 1;
+        }
+    });
+}
+
+// ---- generic FP64 vector helpers ----------------------------------------------------
+__global__ void k_dot(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                      double* part, unsigned int* counter, double* out) {
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        acc[0] += a[i] * b[i];
+    grid_reduce<1>(acc, part, counter, [=](double* t) { *out = t[0]; });
+}
+
+// y = a*x + b*y
+__global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = a * x[i] + b * y[i];
+}
+
+// out = x / d  (pressure preconditioner Ĝ⁻¹ r)
+__global__ void k_div(int64_t n, const double* __restrict__ x, const double* __restrict__ d,
+                      double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = x[i] / d[i];
+}
+
+__global__ void k_to_f32(int64_t n, const double* __restrict__ x, float* __restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = (float)x[i];
+}
+
+// x += (double) e and r = 0, so that a K launch can accumulate K x into r
+__global__ void k_refine_step(int64_t n, const float* __restrict__ e, double* __restrict__ x,
+                              double* __restrict__ r) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += (double)e[i];
+        r[i] = 0.0;
+    }
+}
+
+// r = b − Kx (Kx in r on entry, accumulated by the apply), z-norm partials
+__global__ void k_defect(int64_t n, int64_t nnode, const uint8_t* __restrict__ bcmask,
+                         const double* __restrict__ b, const double* __restrict__ diag,
+                         double* __restrict__ r, double* part, unsigned int* counter, double* out) {
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i / nnode);
+        const bool fixed = (bcmask[i - (int64_t)c * nnode] >> c) & 1;
+        const double rv = fixed ? 0.0 : b[i] - r[i];
+        r[i] = rv;
+        const double zv = fixed ? 0.0 : rv / diag[i];
+        acc[0] += zv * zv;
+    }
+    grid_reduce<1>(acc, part, counter, [=](double* t) { *out = sqrt(t[0]); });
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- host side ----
+struct Scratch {
+    double* part;
+    unsigned int* counter;
+    double* out;
+};
+
+static Scratch scratch(Handle& H) {
+    // [partials 4*kRedBlocks doubles][out 8 doubles][counters 8 uint]
+    H.red.ensure(sizeof(double) * (4 * kRedBlocks + 8) + sizeof(unsigned int) * 8);
+    Scratch s;
+    s.part = H.red.as<double>();
+    s.out = s.part + 4 * kRedBlocks;
+    s.counter = reinterpret_cast<unsigned int*>(s.out + 8);
+    return s;
+}
+
+static void init_scratch(Handle& H) {
+    Scratch s = scratch(H);
+    GG_CUDA(cudaMemsetAsync(s.counter, 0, sizeof(unsigned int) * 8, H.stream));
+    H.scal.ensure(sizeof(KrylovScalars) * 2);
+    if (!H.h_scal) GG_CUDA(cudaMallocHost(&H.h_scal, sizeof(KrylovScalars) * 2));
+}
+
+static double dot(Handle& H, int64_t n, const double* a, const double* b) {
+    Scratch s = scratch(H);
+    k_dot<<<kRedBlocks, 256, 0, H.stream>>>(n, a, b, s.part, s.counter, s.out);
+    GG_CUDA(cudaGetLastError());
+    H.kernel_launches++;
+    double v;
+    GG_CUDA(cudaMemcpyAsync(&v, s.out, sizeof(double), cudaMemcpyDeviceToHost, H.stream));
+    GG_CUDA(cudaStreamSynchronize(H.stream));
+    return v;
+}
+
+static void axpby(Handle& H, int64_t n, double a, const double* x, double b, double* y) {
+    k_axpby<<<grid_for(n, 256), 256, 0, H.stream>>>(n, a, x, b, y);
+    GG_CUDA(cudaGetLastError());
+    H.kernel_launches++;
+}
+
+template <typename V>
+static void cg_iteration_kernels(Handle& H, const MeshK& mk, const V* mom, const uint8_t* bcmask,
+                                 const V* diag, V* x, V* r, V* z, V* p, V* Ap, KrylovScalars* ks,
+                                 Scratch sc) {
+    const int64_t n = (int64_t)mk.dim * mk.nnode;
+    const int ga = apply_grid(mk.nel);
+    if (mk.dim == 2)
+        k_cg_apply<2, V><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter);
+    else
+        k_cg_apply<3, V><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter + 1);
+    k_cg_update<V><<<kRedBlocks, 256, 0, H.stream>>>(n, mk.nnode, bcmask, diag, x, r, z, p, Ap, ks,
+                                                     sc.part, sc.counter + 2);
+    k_cg_direction<V><<<grid_for(n, 256), 256, 0, H.stream>>>(n, z, p, ks);
+}
+
+// Jacobi-preconditioned CG on fixed handle buffers; b and x are device vectors of V.
+template <typename V>
+static int run_cg(Handle& H, const char* key, const MeshK& mk, const V* mom, const V* diag,
+                  const V* b, V* x, V* r, V* z, V* p, V* Ap, double rtol, int maxit, int* iters) {
+    Scratch sc = scratch(H);
+    KrylovScalars* ks = H.scal.as<KrylovScalars>();
+    const int64_t n = (int64_t)mk.dim * mk.nnode;
+    const uint8_t* bcmask = H.bcmask.as<uint8_t>();
+    k_cg_init<V><<<kRedBlocks, 256, 0, H.stream>>>(n, mk.dim, mk.nnode, bcmask, b, diag, x, r, z, p, Ap,
+                                                   rtol, maxit, ks, sc.part,
+                                                   sc.counter + 3);
+    GG_CUDA(cudaGetLastError());
+    H.kernel_launches++;
+    // the graph bakes in every pointer: key it on them
+    char kbuf[160];
+    snprintf(kbuf, sizeof kbuf, "%s:%p:%p:%p:%p:%p", key, (const void*)mom, (const void*)b, (void*)x,
+             (void*)ks, (void*)sc.part);
+    std::string gkey(kbuf);
+    auto it = H.graphs.find(gkey);
+    if (it == H.graphs.end()) {
+        cudaGraph_t g;
+        GG_CUDA(cudaStreamBeginCapture(H.stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < kChunk; k++)
+            cg_iteration_kernels<V>(H, mk, mom, bcmask, diag, x, r, z, p, Ap, ks, sc);
+        GG_CUDA(cudaStreamEndCapture(H.stream, &g));
+        cudaGraphExec_t ge;
+        GG_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        GG_CUDA(cudaGraphDestroy(g));
+        it = H.graphs.emplace(gkey, ge).first;
+    }
+    // every graph launch advances the iteration count by kChunk or sets done, so the
+    // loop ends after at most maxit/kChunk + 1 launches; the guard only protects the host
+    const int64_t max_launches = (int64_t)maxit / kChunk + 4;
+    for (int64_t launches = 0;; launches++) {
+        GG_CUDA(cudaMemcpyAsync(H.h_scal, ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, H.stream));
+        GG_CUDA(cudaStreamSynchronize(H.stream));
+        if (H.h_scal->done) break;
+        if (launches > max_launches) return GG_ERR_NOT_CONVERGED;
+        GG_CUDA(cudaGraphLaunch(it->second, H.stream));
+        GG_CUDA(cudaGetLastError());
+        H.kernel_launches += 3 * kChunk;
+    }
+    *iters = H.h_scal->iterations;
+    if (H.h_scal->failed == 1) return GG_ERR_NOT_CONVERGED;
+    if (H.h_scal->failed) return GG_ERR_NONFINITE;
+    return GG_OK;
+}
+
+void release_graphs(Handle& H) {
+    for (auto& kv : H.graphs) cudaGraphExecDestroy(kv.second);
+    H.graphs.clear();
+}
+
+static void ensure_solver_buffers(Handle& H, bool mixed) {
+    const int64_t nd = H.ndof, ne = H.nel;
+    for (DBuf* b : {&H.u, &H.vstar, &H.ftmp, &H.ub, &H.cg_b, &H.cg_r, &H.cg_z, &H.cg_p, &H.cg_Ap, &H.cg_x})
+        b->ensure(sizeof(double) * nd);
+    for (DBuf* b : {&H.q, &H.qtmp, &H.r, &H.s}) b->ensure(sizeof(double) * ne);
+    if (mixed)
+        for (DBuf* b : {&H.r32, &H.cgr32, &H.z32, &H.p32, &H.Ap32, &H.e32}) b->ensure(sizeof(float) * nd);
+    init_scratch(H);
+}
+
+// x = K⁻¹ b (device FP64 vectors), stopping rule of the reference's inner KSP.
+int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* x, double rtol,
+                int maxit, int* iters) {
+    const int64_t nd = H.ndof;
+    const uint8_t* bcmask = H.bcmask.as<uint8_t>();
+    if (prm.precision == GG_PRECISION_FP64) {
+        GG_CUDA(cudaMemcpyAsync(H.cg_b.p, b, sizeof(double) * nd, cudaMemcpyDeviceToDevice, H.stream));
+        int rc = run_cg<double>(H, "cg64", H.mk, H.mom64.as<double>(), H.kdiag64.as<double>(),
+                                H.cg_b.as<double>(), H.cg_x.as<double>(), H.cg_r.as<double>(),
+                                H.cg_z.as<double>(), H.cg_p.as<double>(), H.cg_Ap.as<double>(), rtol,
+                                maxit, iters);
+        GG_CUDA(cudaMemcpyAsync(x, H.cg_x.p, sizeof(double) * nd, cudaMemcpyDeviceToDevice, H.stream));
+        return rc;
+    }
+    // ---- mixed: FP64 defect correction around FP32 Jacobi CG
+    Scratch sc = scratch(H);
+    double* r64 = H.cg_r.as<double>();
+    double* bb = H.cg_b.as<double>();
+    GG_CUDA(cudaMemcpyAsync(bb, b, sizeof(double) * nd, cudaMemcpyDeviceToDevice, H.stream));
+    GG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * nd, H.stream));
+    // rnorm0 = ‖D⁻¹ b‖ on free rows
+    GG_CUDA(cudaMemsetAsync(r64, 0, sizeof(double) * nd, H.stream));
+    k_defect<<<kRedBlocks, 256, 0, H.stream>>>(nd, H.nnode, bcmask, bb, H.kdiag64.as<double>(), r64,
+                                                sc.part, sc.counter + 4, sc.out + 1);
+    double rnorm0;
+    GG_CUDA(cudaMemcpyAsync(&rnorm0, sc.out + 1, sizeof(double), cudaMemcpyDeviceToHost, H.stream));
+    GG_CUDA(cudaStreamSynchronize(H.stream));
+    double ttol = rtol * rnorm0;
+    if (ttol < 1e-50) ttol = 1e-50;
+    int total = 0;
+    if (rnorm0 <= ttol) { *iters = 0; return GG_OK; }
+    const double inner_rtol = 1e-3;
+    for (int sweep = 0; sweep < 50; sweep++) {
+        k_to_f32<<<grid_for(nd, 256), 256, 0, H.stream>>>(nd, r64, H.r32.as<float>());
+        int it = 0;
+        int rc = run_cg<float>(H, "cg32", H.mk, H.mom32.as<float>(), H.kdiag32.as<float>(), H.r32.as<float>(),
+                               H.e32.as<float>(), H.cgr32.as<float>(), H.z32.as<float>(), H.p32.as<float>(),
+                               H.Ap32.as<float>(), inner_rtol, maxit, &it);
+        total += it;
+        if (rc == GG_ERR_NONFINITE) return rc;
+        // x += e ; r = b − K64 x
+        k_refine_step<<<grid_for(nd, 256), 256, 0, H.stream>>>(nd, H.e32.as<float>(), x, r64);
+        apply_K<double>(H.mk, H.mom64.as<double>(), bcmask, x, r64, H.stream);
+        k_defect<<<kRedBlocks, 256, 0, H.stream>>>(nd, H.nnode, bcmask, bb, H.kdiag64.as<double>(), r64,
+                                                    sc.part, sc.counter + 4, sc.out + 1);
+        double rn;
+        GG_CUDA(cudaMemcpyAsync(&rn, sc.out + 1, sizeof(double), cudaMemcpyDeviceToHost, H.stream));
+        GG_CUDA(cudaStreamSynchronize(H.stream));
+        if (!(rn == rn)) return GG_ERR_NONFINITE;
+        if (rn <= ttol) { *iters = total; return GG_OK; }
+        if (total >= maxit) break;
+    }
+    *iters = total;
+    return GG_ERR_NOT_CONVERGED;
+}
+
+int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
+    const bool mixed = prm.precision == GG_PRECISION_MIXED;
+    ensure_solver_buffers(H, mixed);
+    std::memset(&S, 0, sizeof S);
+    cudaStream_t st = H.stream;
+    const int64_t nd = H.ndof, ne = H.nel;
+    double* f = H.f.as<double>();
+    double* hv = H.hvec.as<double>();
+    double* u = H.u.as<double>();
+    double* vstar = H.vstar.as<double>();
+    double* ftmp = H.ftmp.as<double>();
+    double* q = H.q.as<double>();      // pressure (solution)
+    double* qtmp = H.qtmp.as<double>();
+    double* r = H.r.as<double>();
+    double* s = H.s.as<double>();
+    const int maxit = prm.inner_max_iterations > 0 ? prm.inner_max_iterations : 10000;
+    GG_CUDA(cudaEventRecord(H.ev0, st));
+    const int64_t launches0 = H.kernel_launches;
+    int64_t nfree = H.nfree;
+    const double scaleq = sqrt((double)ne);
+    int rc = GG_OK, it = 0;
+    auto inner = [&](const double* b, double* x, double rtol) {
+        int its = 0;
+        int r2 = inner_solve(H, prm, b, x, rtol, maxit, &its);
+        S.inner_iterations += its;
+        S.inner_solves++;
+        return r2;
+    };
+    const double fnorm = sqrt(dot(H, nd, f, f));
+    if (fnorm / sqrt((double)nfree) <= 1e-99) return GG_ERR_ZERO_FORCE;
+    // STEP 1 (:553-565)
+    if ((rc = inner(f, vstar, prm.tolerance)) != GG_OK) return rc;
+    apply_GT(H, vstar, qtmp, st);
+    axpby(H, ne, -1.0, hv, 1.0, qtmp);
+    const double inner_rtol = prm.inner_rtol_factor * prm.tolerance;
+    const double rhs_scale = sqrt(dot(H, ne, qtmp, qtmp)) / scaleq;
+    if (!isfinite(rhs_scale)) return GG_ERR_NONFINITE;
+    // STEP 3 (:616-659)
+    apply_G(H, q, ftmp, st);
+    axpby(H, nd, 1.0, f, -1.0, ftmp);
+    if ((rc = inner(ftmp, u, inner_rtol)) != GG_OK) return rc;
+    apply_GT(H, u, r, st);
+    axpby(H, ne, -1.0, hv, 1.0, r);
+    // STEP 4 (:664-837)
+    double zr_prev = 1.0, absres = 0.0, relres = 0.0;
+    for (;;) {
+        if (prm.use_preconditioner) {
+            k_div<<<grid_for(ne, 256), 256, 0, st>>>(ne, r, H.sdiag.as<double>(), qtmp);
+            H.kernel_launches++;
+        } else {
+            GG_CUDA(cudaMemcpyAsync(qtmp, r, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
+        }
+        const double zr = dot(H, ne, qtmp, r);
+        if (it == 0)
+            GG_CUDA(cudaMemcpyAsync(s, qtmp, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
+        else
+            axpby(H, ne, 1.0, qtmp, zr / zr_prev, s);
+        apply_G(H, s, ftmp, st);
+        if ((rc = inner(ftmp, vstar, inner_rtol)) != GG_OK) return rc;
+        apply_GT(H, vstar, qtmp, st);
+        const double sq = dot(H, ne, s, qtmp);
+        const double alpha = zr / sq;
+        if (!isfinite(zr) || !isfinite(sq) || !isfinite(alpha)) return GG_ERR_NONFINITE;
+        axpby(H, ne, alpha, s, 1.0, q);
+        axpby(H, nd, -alpha, vstar, 1.0, u);
+        axpby(H, ne, -alpha, qtmp, 1.0, r);
+        zr_prev = zr;
+        absres = sqrt(dot(H, ne, r, r)) / scaleq;
+        relres = absres / rhs_scale;
+        if (!isfinite(absres)) return GG_ERR_NONFINITE;
+        if (!(it < prm.max_iterations)) { rc = GG_ERR_NOT_CONVERGED; it++; break; }
+        it++;
+        const double chosen = prm.use_absolute_tolerance ? absres : relres;
+        if (!((chosen > prm.tolerance) || (it < prm.min_iterations))) break;
+    }
+    S.outer_iterations = it;
+    S.kernel_launches = H.kernel_launches - launches0;
+    S.rel_residual = relres;
+    S.abs_residual = absres;
+    GG_CUDA(cudaEventRecord(H.ev1, st));
+    // summary norms (:844-877), outside the timed region
+    apply_GT(H, u, qtmp, st);
+    const double un = sqrt(dot(H, nd, u, u));
+    S.div_u = sqrt(dot(H, ne, qtmp, qtmp)) / un;
+    apply_G(H, q, vstar, st);
+    GG_CUDA(cudaMemsetAsync(ftmp, 0, sizeof(double) * nd, st));
+    apply_K<double>(H.mk, H.mom64.as<double>(), H.bcmask.as<uint8_t>(), u, ftmp, st);
+    axpby(H, nd, 1.0, vstar, 1.0, ftmp);
+    axpby(H, nd, 1.0, f, -1.0, ftmp);
+    S.momentum_residual = sqrt(dot(H, nd, ftmp, ftmp)) / fnorm;
+    float ms = 0.f;
+    GG_CUDA(cudaEventSynchronize(H.ev1));
+    GG_CUDA(cudaEventElapsedTime(&ms, H.ev0, H.ev1));
+    S.solve_ms = ms;
+    return rc;
+}
+
+}  // namespace gg

@@ -1,0 +1,281 @@
+/*
+ * gale_gpu.h -- C ABI of the B200 (sm_100a) particle-in-cell Q1-P0 Stokes path.
+ *
+ * One opaque handle owns one regular Cartesian Q1 velocity / P0 pressure mesh, its
+ * material-point swarm and every device buffer.  The host passes plain pointers that
+ * are valid for the duration of the call only; the library copies in and out.  Every
+ * entry point returns an int status (GG_OK == 0, negative on error) and never aborts;
+ * gg_last_error() gives the message.  The reference reports the same failures through
+ * Journal_Firewall (abort); the host plugin maps a non-zero status back onto it.
+ *
+ * Conventions shared with the reference (StgFEM / StgDomain / PICellerator):
+ *   - element index  e = i + nx*(j + ny*k)            (Grid_Project, StgDomain/Mesh/src/Grid.cxx:254-272)
+ *   - node index     n = i + (nx+1)*(j + (ny+1)*k)
+ *   - element-local node a has offsets (a&1, (a>>1)&1, (a>>2)&1)
+ *                                          (BilinearElementType.cxx:216-245, TrilinearElementType.cxx:257-300)
+ *   - nodal vectors are node-major, dim components per node (FeVariable dof layout)
+ *   - y (J_AXIS) is the vertical axis; gravity and thermal buoyancy act along it.
+ *
+ * Not re-entrant per handle.  One CUDA stream per handle.
+ */
+#ifndef GALE_GPU_H
+#define GALE_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GG_API __attribute__((visibility("default")))
+#else
+#define GG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------ */
+enum {
+    GG_OK                 = 0,
+    GG_ERR_INVALID        = -1,  /* bad argument or size                              */
+    GG_ERR_CUDA           = -2,  /* CUDA runtime error (message in gg_last_error)     */
+    GG_ERR_NONFINITE      = -3,  /* NaN/Inf in a solver scalar (isGoodNumber firewall) */
+    GG_ERR_NOT_CONVERGED  = -4,  /* iteration cap reached                             */
+    GG_ERR_STAGNATED      = -5,  /* learned preconditioner stagnated and no fallback  */
+    GG_ERR_OUT_OF_DOMAIN  = -6,  /* a material point lies outside the mesh            */
+    GG_ERR_ZERO_FORCE     = -7,  /* momentum force vector is zero                     */
+    GG_ERR_STATE          = -8,  /* entry point called before its inputs were set     */
+    GG_ERR_NO_DEVICE      = -9,  /* no CUDA device                                    */
+    GG_ERR_EMPTY_CELL     = -10  /* an element holds no material point                */
+};
+
+/* ---- mesh ---------------------------------------------------------------------- */
+typedef struct gg_mesh_desc {
+    int32_t dim;          /* 2 or 3                                  */
+    int32_t elements[3];  /* elementResI/J/K                         */
+    double  min[3];       /* minX/minY/minZ                          */
+    double  max[3];       /* maxX/maxY/maxZ                          */
+} gg_mesh_desc;
+
+/* ---- velocity boundary conditions (WallVC) -------------------------------------
+ * wall order: 0 left (min x), 1 right (max x), 2 bottom (min y), 3 top (max y),
+ *             4 back (min z), 5 front (max z).  A node on several walls takes the
+ *             value of the last wall in this order that fixes the component.     */
+typedef struct gg_velocity_bc {
+    uint8_t fixed[6][3];
+    double  value[6][3];
+} gg_velocity_bc;
+
+/* ---- rheology (Underworld/Rheology) -------------------------------------------- */
+enum {
+    GG_RHEO_MATERIAL_VISCOSITY = 1, /* MaterialViscosity.cxx:129-149                  */
+    GG_RHEO_ARRHENIUS          = 2, /* Arrhenius.cxx:170-220                          */
+    GG_RHEO_FRANK_KAMENETSKII  = 3, /* FrankKamenetskii.cxx:143-161                   */
+    GG_RHEO_VON_MISES          = 4, /* VonMises.cxx:183-289                           */
+    GG_RHEO_DRUCKER_PRAGER     = 5, /* DruckerPrager.cxx:296-490                      */
+    GG_RHEO_BYERLEE            = 6  /* Byerlee.cxx:163-187                            */
+};
+
+#define GG_MAX_RHEOLOGIES 4
+#define GG_MAX_MATERIALS  16
+
+typedef struct gg_rheology {
+    int32_t kind;                       /* GG_RHEO_*                                  */
+    int32_t strain_weakening;           /* 1: uses the material's StrainWeakening     */
+    /* creep laws */
+    double eta0;
+    double activation_energy;           /* Arrhenius                                  */
+    double activation_volume;           /* Arrhenius                                  */
+    double reference_temp;              /* Arrhenius                                  */
+    double theta;                       /* FrankKamenetskii                           */
+    /* yield laws */
+    double cohesion;
+    double cohesion_after_softening;
+    double friction_coefficient;        /* DruckerPrager                              */
+    double friction_coefficient_after_softening;
+    double minimum_yield_stress;        /* DruckerPrager                              */
+    double minimum_viscosity;           /* YieldRheology minimumViscosity             */
+    double max_strain_rate;             /* DruckerPrager                              */
+    double depth_coefficient;           /* Byerlee                                    */
+    int32_t strain_rate_softening;      /* VonMises                                   */
+    int32_t pad;
+} gg_rheology;
+
+typedef struct gg_strain_weakening {    /* StrainWeakening.cxx:250-275                */
+    double initial_softening_strain;
+    double final_softening_strain;
+    double healing_rate;
+} gg_strain_weakening;
+
+typedef struct gg_material {
+    int32_t n_rheologies;               /* run in order (Rheology_Register.cxx:70-86) */
+    int32_t has_strain_weakening;
+    gg_rheology rheology[GG_MAX_RHEOLOGIES];
+    gg_strain_weakening strain_weakening;
+    double density;                     /* BuoyancyForceTerm density                  */
+    double alpha;                       /* BuoyancyForceTerm thermal expansivity      */
+} gg_material;
+
+/* ---- body force ------------------------------------------------------------------ */
+typedef struct gg_body_force {
+    double gravity;        /* BuoyancyForceTerm: f += gravity*gHat*rho*N*w*detJ      */
+    double g_hat[3];       /* unit direction (normalised by the library)            */
+    double rayleigh;       /* ThermalBuoyancyForceTerm: f_y += Ra*T*N*w*detJ (0=off)  */
+} gg_body_force;
+
+/* ---- solver configuration ------------------------------------------------------ */
+enum {
+    GG_PRECISION_FP64  = 0,  /* every operator and vector in FP64                      */
+    GG_PRECISION_MIXED = 1   /* FP32 viscosity, moments and inner K applies inside FP64
+                                iterative refinement; FP64 Uzawa update, Schur residual,
+                                dots and r = b - A x                                     */
+};
+enum {
+    GG_INNER_JACOBI_CG  = 0, /* PETSc -ksp_type cg -pc_type jacobi                     */
+    GG_INNER_MG_CG      = 1, /* geometric multigrid V-cycle preconditioned CG          */
+    GG_INNER_LEARNED_CG = 2  /* MG + learned coarse correction, flexible CG; falls back
+                                to GG_INNER_MG_CG when the residual stagnates          */
+};
+
+typedef struct gg_uzawa_params {
+    double  tolerance;            /* Stokes_SLE_UzawaSolver "tolerance" (1e-5)          */
+    int32_t max_iterations;       /* "maxIterations" (1000)                             */
+    int32_t min_iterations;       /* "minIterations" (1)                                */
+    int32_t use_absolute_tolerance;
+    int32_t use_preconditioner;   /* Ĝ = Gᵀ diag(K_e)⁻¹ G pressure preconditioner       */
+    int32_t inner;                /* GG_INNER_*                                         */
+    int32_t precision;            /* GG_PRECISION_*                                     */
+    double  inner_rtol_factor;    /* inner rtol = factor*tolerance (0.1)                */
+    int32_t inner_max_iterations; /* per inner solve (PETSc default 10000)              */
+    int32_t reuse_pressure;       /* start from the p passed in (Picard, restart)       */
+} gg_uzawa_params;
+
+typedef struct gg_uzawa_stats {
+    int32_t outer_iterations;
+    int32_t inner_iterations;     /* total inner Krylov iterations (all solves)         */
+    int32_t inner_solves;
+    int32_t fallbacks;            /* learned → MG fallbacks taken                       */
+    double  rel_residual;         /* final Uzawa relResidual                            */
+    double  abs_residual;
+    double  div_u;                /* |Gᵀu|/|u|                                          */
+    double  momentum_residual;    /* |f - K u - G p| / |f|                              */
+    double  solve_ms;             /* device time of the solve                           */
+    int64_t kernel_launches;      /* launches of this library's kernels in the solve    */
+} gg_uzawa_stats;
+
+typedef struct gg_picard_params {
+    int32_t max_iterations;       /* nonLinearMaxIterations                             */
+    int32_t min_iterations;       /* nonLinearMinIterations                             */
+    double  tolerance;            /* nonLinearTolerance                                 */
+} gg_picard_params;
+
+typedef struct gg_picard_stats {
+    int32_t iterations;
+    int32_t converged;
+    double  residual;             /* ‖u_k − u_{k−1}‖ / ‖u_k‖ at exit                     */
+    int32_t outer_iterations;     /* Uzawa iterations over all Picard steps              */
+    int32_t inner_iterations;
+    double  solve_ms;
+} gg_picard_stats;
+
+typedef struct gg_handle gg_handle;
+
+/* ---- lifetime -------------------------------------------------------------------
+ * Replaces the Stokes_SLE_UzawaSolver object lifetime: _Build
+ * (StgFEM/SLE/ProvidedSystems/StokesFlow/src/Stokes_SLE_UzawaSolver.cxx:199-239) and
+ * _Destroy (:269-287).                                                               */
+GG_API int  gg_create(const gg_mesh_desc* mesh, gg_handle** out);
+GG_API int  gg_destroy(gg_handle* h);
+GG_API const char* gg_last_error(const gg_handle* h);
+GG_API const char* gg_version(void);
+
+/* ---- inputs ---------------------------------------------------------------------- */
+/* Velocity BCs: the WallVC/CompositeVC "velocityBCs" of VelocityField (FeVariable_IsBC,
+ * StgFEM/Discretisation/src/FeVariable.cxx) as consumed by __StiffnessMatrix_NewAssemble
+ * (StgFEM/SLE/SystemSetup/src/StiffnessMatrix.cxx:2091-2143).                          */
+GG_API int  gg_set_velocity_bc(gg_handle* h, const gg_velocity_bc* bc);
+/* Material table: RheologyMaterial + its Rheology_Register
+ * (Underworld/Rheology/src/Rheology_Register.cxx:70-86), density/alpha of
+ * BuoyancyForceTerm (PICellerator/Utils/src/BuoyancyForceTerm.cxx:414-530).           */
+GG_API int  gg_set_materials(gg_handle* h, int32_t n_materials, const gg_material* materials);
+/* Material points: MaterialPointsSwarm coords (StandardParticle.h:52-80), material
+ * index (MaterialPoint.h:48-52) and StrainWeakening postFailureWeakening (nullable).  */
+GG_API int  gg_set_points(gg_handle* h, int64_t n_points, const double* coords,
+                   const int32_t* material, const double* plastic_strain);
+/* Nodal temperature of TemperatureField (nullable: no temperature).                   */
+GG_API int  gg_set_temperature(gg_handle* h, const double* nodal_temperature);
+GG_API int  gg_set_body_force(gg_handle* h, const gg_body_force* force);
+
+/* ---- point → cell, ξ, weights ------------------------------------------------------
+ * Replaces Swarm_UpdateAllParticleOwners (StgDomain/Swarm/src/SwarmClass.cxx:878-992)
+ * with Mesh_RegularAlgorithms_SearchElements (StgDomain/Mesh/src/
+ * Mesh_RegularAlgorithms.cxx:191-224) as the search, _CoincidentMapper_Map
+ * (PICellerator/MaterialPoints/src/CoincidentMapper.cxx:158-240) for ξ and the
+ * per-cell tables, and _ConstantWeights_Calculate (PICellerator/Weights/src/
+ * ConstantWeights.cxx:178-187).  owning_cell (nullable) receives the element of each
+ * point, bit-exact with the reference; points outside the mesh return
+ * GG_ERR_OUT_OF_DOMAIN and get cell = element count (ElementCellLayout.cxx:266-275). */
+GG_API int  gg_locate(gg_handle* h, uint32_t* owning_cell);
+
+/* ---- operator build ---------------------------------------------------------------
+ * Replaces the assembleStiffnessMatrix entry point (__StiffnessMatrix_NewAssemble,
+ * StiffnessMatrix.cxx:2016-2200) for k_matrix, g_matrix and the Uzawa preconditioner,
+ * i.e. _ConstitutiveMatrixCartesian_AssembleElement (Underworld/Rheology/src/
+ * ConstitutiveMatrixCartesian.cxx:206-487), _GradientStiffnessMatrixTerm_AssembleElement
+ * (StgFEM/Assembly/src/GradientStiffnessMatrixTerm.cxx:161-251) and
+ * _UzawaPreconditionerTerm_AssembleElement (StgFEM/SLE/ProvidedSystems/StokesFlow/src/
+ * UzawaPreconditionerTerm.cxx:156-239), plus the force vector terms.  Per point runs
+ * the rheology chain; per element stores the viscosity moments of the PIC quadrature.
+ * previous_solution_exists gates yielding (YieldRheology.cxx:203-204); u and p
+ * (nodal velocity, element pressure, nullable when it is 0) are the previous solution
+ * the yield laws read.                                                                */
+GG_API int  gg_build_operator(gg_handle* h, int32_t precision, int32_t previous_solution_exists,
+                       const double* u, const double* p);
+
+/* ---- solve ---------------------------------------------------------------------------
+ * Replaces _Stokes_SLE_UzawaSolver_Solve (Stokes_SLE_UzawaSolver.cxx:393-938) with its
+ * inner velocity KSP.  u: nodal velocity [nodes*dim] (out; BC dofs carry their values),
+ * p: element pressure [elements] (in when reuse_pressure, out).                        */
+GG_API int  gg_uzawa_solve(gg_handle* h, const gg_uzawa_params* params, double* u, double* p,
+                    gg_uzawa_stats* stats);
+
+/* Replaces SystemLinearEquations_NonLinearExecute (StgFEM/SLE/SystemSetup/src/
+ * SystemLinearEquations.cxx:735-920) for the Stokes SLE: operator build + Uzawa per
+ * iteration, yielding enabled from the second solve.                                   */
+GG_API int  gg_picard(gg_handle* h, const gg_picard_params* picard, const gg_uzawa_params* uzawa,
+               double* u, double* p, gg_picard_stats* stats);
+
+/* ---- advection ---------------------------------------------------------------------
+ * Replaces TimeIntegrand_SecondOrder / first order (StgDomain/Utils/src/
+ * TimeIntegrand.cxx:265-335, :457-483) with _SwarmAdvector_TimeDeriv
+ * (PICellerator/MaterialPoints/src/SwarmAdvector.cxx:261-287) as the derivative, on the
+ * handle's points and the velocity of the last solve (or u when non-null).  Points keep
+ * their order.  coords_out (nullable) receives the advected coordinates.              */
+GG_API int  gg_advect(gg_handle* h, double dt, int32_t order, const double* u, double* coords_out);
+/* Stokes_SLE_UpdateDt (StgFEM/SLE/ProvidedSystems/StokesFlow/src/UpdateDt.cxx:53-84):
+ * dt = 0.5 * min element separation / max |v| over velocity nodes.                    */
+GG_API int  gg_courant_dt(gg_handle* h, const double* u, double* dt);
+
+/* ---- diagnostics and operator access (parity tests, host shims) ---------------------- */
+/* Per-point viscosity η of the last operator build, in input point order.             */
+GG_API int  gg_get_point_viscosity(gg_handle* h, double* eta);
+/* Per-point StrainWeakening increment and yield flag of the last build (nullable).    */
+GG_API int  gg_get_point_yield(gg_handle* h, double* increment, uint8_t* yielded);
+/* Element moments M_m(e) = Σ_p w_p detJ η_p m(ξ_p) in FP64, [n_moments][elements].    */
+GG_API int  gg_get_moments(gg_handle* h, double* moments, int32_t* n_moments);
+/* y = K x on free dofs (BC rows and columns removed, as the reduced PETSc matrix).    */
+GG_API int  gg_apply_K(gg_handle* h, int32_t precision, const double* x, double* y);
+/* y = G p (velocity sized, BC rows zero);  q = Gᵀ u (element sized, BC columns zero). */
+GG_API int  gg_apply_G(gg_handle* h, const double* p, double* y);
+GG_API int  gg_apply_GT(gg_handle* h, const double* u, double* q);
+/* Force vectors after BC elimination: f [nodes*dim], h [elements].                   */
+GG_API int  gg_get_rhs(gg_handle* h, double* f, double* hvec);
+/* Diagonal of the assembled K [nodes*dim] and of Ĝ [elements].                        */
+GG_API int  gg_get_diagonals(gg_handle* h, double* k_diag, double* schur_diag);
+/* Measurement only (no reference counterpart): average device time of one matrix-free
+ * K apply over `reps` back-to-back launches on the handle's stream, CUDA events.       */
+GG_API int  gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GALE_GPU_H */

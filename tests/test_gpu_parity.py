@@ -1,0 +1,256 @@
+"""Parity of the sm_100a path with the CPU oracle, through the C ABI (needs a B200).
+
+Bars: bit-exact for the integer point→element mapping; ≤1e-12 relative for FP64
+operators (K, G, Gᵀ, RHS, diagonals, moments, viscosity); ≤1e-10 relative L2 for the
+plain FP64 Uzawa solution at tight tolerance; the mixed FP32/FP64 solution within the
+stated 1e-5 relative L2 of the FP64 oracle solution at the same Uzawa tolerance.
+"""
+import numpy as np
+import pytest
+
+from gale_b200 import abi, workloads
+from gale_b200.stokes import StokesProblem, UzawaSolver, GaleError, Mesh, MaterialViscosity, \
+    RheologyMaterial, free_slip, BodyForce
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
+
+
+def pair(w, oracle_mod):
+    G = w.apply(StokesProblem(w.mesh))
+    O = w.apply(oracle_mod.OracleProblem(w.mesh))
+    return G, O
+
+
+# ---------------------------------------------------------------- point → cell ----
+def edge_points(mesh, rng, n=20000):
+    """Points on and within 1e-13/1e-11 of element faces, on the walls and outside."""
+    dim = mesh.dim
+    pts = []
+    for d in range(dim):
+        v = workloads.vertex_coords(mesh, d)
+        pts.append(v)
+    base = rng.uniform(0, 1, size=(n, dim))
+    for d in range(dim):
+        lo, hi = mesh.min[d], mesh.max[d]
+        base[:, d] = lo + base[:, d] * (hi - lo)
+    # snap a third of each coordinate to a vertex, then nudge some by ±1e-13/±1e-11
+    for d in range(dim):
+        v = pts[d]
+        k = rng.integers(0, 3, size=n)
+        snap = v[rng.integers(0, len(v), size=n)]
+        nudge = rng.choice([0.0, 1e-13, -1e-13, 5e-12, -5e-12, 1e-11, -1e-11], size=n)
+        base[:, d] = np.where(k == 0, snap + nudge, base[:, d])
+    # walls exactly, and a few outside
+    base[:50, 0] = mesh.max[0]
+    base[50:100, 0] = mesh.min[0]
+    base[100:110, 0] = mesh.max[0] + 1e-9
+    base[110:120, 1] = mesh.min[1] - 1e-9
+    return np.ascontiguousarray(base)
+
+
+@pytest.mark.parametrize("dim,elements,lo,hi", [
+    (2, (64, 64), (0.0, 0.0), (1.0, 1.0)),
+    (2, (256, 64), (0.0, 0.0), (4.0, 1.0)),
+    (3, (16, 12, 10), (-1.0, 0.0, 0.5), (1.0, 0.7, 2.0)),
+])
+def test_locate_bit_exact(oracle_mod, dim, elements, lo, hi):
+    mesh = Mesh(dim, elements, lo, hi)
+    rng = np.random.default_rng(1)
+    x = edge_points(mesh, rng)
+    expect = oracle_mod.locate(mesh, x)
+    G = StokesProblem(mesh)
+    G.set_materials([RheologyMaterial([MaterialViscosity(1.0)])])
+    G.set_points(x)
+    with pytest.raises(GaleError) as ei:
+        G.locate()
+    assert ei.value.code == abi.GG_ERR_OUT_OF_DOMAIN
+    import ctypes as C
+    cell = np.empty(x.shape[0], dtype=np.uint32)
+    G.lib.gg_locate(G.h, cell.ctypes.data_as(C.POINTER(C.c_uint32)))
+    assert np.array_equal(cell, expect)
+    nel = int(np.prod(elements))
+    # the 20 planted outside points, plus wall points nudged outward by more than 1e-12
+    assert (expect == nel).sum() >= 20
+    assert (expect < nel).sum() > 0.9 * x.shape[0]
+
+
+def test_locate_full_size_sorted_counts(oracle_mod):
+    # C5-sized index space (128×64×128 elements), 2M points: cells and per-cell counts
+    mesh = Mesh(3, (128, 64, 128), (0, 0, 0), (2, 1, 2))
+    rng = np.random.default_rng(3)
+    x = np.ascontiguousarray(rng.uniform(0, 1, size=(2_000_000, 3)) * np.array([2, 1, 2]))
+    G = StokesProblem(mesh)
+    G.set_materials([RheologyMaterial([MaterialViscosity(1.0)])])
+    G.set_points(x)
+    cell = G.locate()
+    assert np.array_equal(cell, oracle_mod.locate(mesh, x))
+
+
+# ----------------------------------------------------------- operator parity ----
+@pytest.mark.parametrize("make", [
+    lambda: workloads.sinker_2d(n=16),
+    lambda: workloads.creep_3d(n=6),
+    lambda: workloads.extension_2d(nx=16, ny=4, ppc=12),
+    lambda: workloads.subduction_3d(nx=8, ny=4, nz=8, ppc=8),
+], ids=["sinker", "creep", "extension", "subduction"])
+def test_operator_parity(oracle_mod, make):
+    w = make()
+    G, O = pair(w, oracle_mod)
+    assert np.array_equal(G.locate(), oracle_mod.locate(w.mesh, w.coords))
+    G.build_operator("mixed")
+    O.assemble()
+    assert rel(G.point_viscosity(), O.point_viscosity()) < 1e-13
+    assert rel(G.moments(), O.moments()) < 1e-12
+    rng = np.random.default_rng(0)
+    for _ in range(3):
+        x = rng.standard_normal(G.nnode * G.dim)
+        y0 = O.apply_K(x)
+        assert rel(G.apply_K(x), y0) < 1e-12
+        assert rel(G.apply_K(x, "mixed"), y0) < 1e-5
+        p = rng.standard_normal(G.nel)
+        assert rel(G.apply_G(p), O.apply_G(p)) < 1e-13
+        assert rel(G.apply_GT(x), O.apply_GT(x)) < 1e-13
+    fg, hg = G.rhs()
+    fo, ho = O.rhs()
+    assert rel(fg, fo) < 1e-12
+    if np.linalg.norm(ho) > 0:
+        assert rel(hg, ho) < 1e-12
+    kg, sg = G.diagonals()
+    ko, so = O.diagonals()
+    assert rel(kg, ko) < 1e-12
+    assert rel(sg, so) < 1e-12
+
+
+def test_yield_parity(oracle_mod):
+    # Drucker-Prager with strain weakening, evaluated on a previous solution
+    w = workloads.extension_2d(nx=32, ny=8, ppc=20)
+    G, O = pair(w, oracle_mod)
+    G.locate()
+    O.assemble()
+    u, p, _ = O.uzawa(UzawaSolver(tolerance=1e-8))
+    G.build_operator("fp64", previous_solution=(u, p))
+    O.assemble(True, u, p)
+    eg, eo = G.point_viscosity(), O.point_viscosity()
+    assert rel(eg, eo) < 1e-12
+    ig, yg = G.point_yield()
+    io, yo = O.point_yield()
+    assert np.array_equal(yg, yo)
+    assert yo.sum() > 0  # the upper crust yields
+    assert rel(ig, io) < 1e-12
+
+
+# -------------------------------------------------------------------- solves ----
+def test_uzawa_tight_fp64(oracle_mod):
+    w = workloads.sinker_2d(n=16)
+    G, O = pair(w, oracle_mod)
+    G.locate()
+    G.build_operator("fp64")
+    O.assemble()
+    prm = UzawaSolver(tolerance=1e-11, innerRtolFactor=0.01)
+    ug, pg, sg = G.solve(prm)
+    uo, po, so = O.uzawa(prm)
+    assert rel(ug, uo) < 1e-10
+    assert rel(pg - pg.mean(), po - po.mean()) < 1e-10
+
+
+def test_uzawa_reference_tolerance_fp64(oracle_mod):
+    # same algorithm and stopping rules: same iteration counts, tolerance-level agreement
+    w = workloads.sinker_2d(n=32)
+    G, O = pair(w, oracle_mod)
+    G.locate()
+    G.build_operator("fp64")
+    O.assemble()
+    ug, pg, sg = G.solve(w.uzawa)
+    uo, po, so = O.uzawa(w.uzawa)
+    assert abs(sg["outer_iterations"] - so["outer_iterations"]) <= 1
+    assert sg["rel_residual"] <= w.uzawa.tolerance
+    assert rel(ug, uo) < 1e-4
+
+
+def test_uzawa_mixed_precision(oracle_mod):
+    w = workloads.creep_3d(n=8)
+    G, O = pair(w, oracle_mod)
+    G.locate()
+    G.build_operator("mixed")
+    O.assemble()
+    tight = UzawaSolver(tolerance=1e-10, innerRtolFactor=0.01)
+    uo, po, _ = O.uzawa(tight)
+    ug, pg, sg = G.solve(UzawaSolver(tolerance=1e-6, precision="mixed"))
+    assert sg["rel_residual"] <= 1e-6
+    assert rel(ug, uo) < 1e-5
+    assert rel(pg - pg.mean(), po - po.mean()) < 1e-5
+
+
+def test_picard_parity(oracle_mod):
+    w = workloads.extension_2d(nx=16, ny=4, ppc=12, picard_its=4)
+    G, O = pair(w, oracle_mod)
+    G.locate()
+    prm = UzawaSolver(tolerance=1e-9, innerRtolFactor=0.01)
+    ug, pg, sg = G.picard(w.picard, prm)
+    uo, po, so = O.picard(w.picard, prm)
+    assert sg["iterations"] == so["iterations"]
+    assert rel(ug, uo) < 1e-7
+
+
+# ----------------------------------------------------------------- advection ----
+def test_advect_rk2_parity(oracle_mod):
+    w = workloads.sinker_2d(n=16)
+    G, O = pair(w, oracle_mod)
+    G.locate()
+    G.build_operator("fp64")
+    O.assemble()
+    u, p, _ = O.uzawa(UzawaSolver(tolerance=1e-8))
+    dt = O.courant_dt(u)
+    assert abs(G.courant_dt(u) - dt) <= 1e-15 * dt
+    xg = G.advect(dt * 40.0, u)  # large step: some corrector positions leave the mesh
+    xo = O.advect(dt * 40.0, u)
+    assert np.max(np.abs(xg - xo)) < 1e-13
+    assert np.array_equal(oracle_mod.locate(w.mesh, xg), oracle_mod.locate(w.mesh, xo))
+
+
+# ------------------------------------------------------------ failure paths ----
+def test_failure_statuses():
+    mesh = Mesh(2, (4, 4))
+    G = StokesProblem(mesh)
+    G.set_materials([RheologyMaterial([MaterialViscosity(1.0)], density=1.0)])
+    G.set_velocity_bc(free_slip(2))
+    rng = np.random.default_rng(0)
+    x = np.ascontiguousarray(rng.uniform(0, 1, size=(400, 2)))
+    # no body force → zero force vector (Stokes_SLE_UzawaSolver.cxx:476-495 firewall)
+    G.set_points(x)
+    G.locate()
+    G.build_operator()
+    with pytest.raises(GaleError) as e:
+        G.solve(UzawaSolver())
+    assert e.value.code == abi.GG_ERR_ZERO_FORCE
+    # iteration cap of 1 → not converged
+    G.set_body_force(BodyForce(gravity=1.0))
+    G.set_materials([RheologyMaterial([MaterialViscosity(1.0)], density=1.0),
+                     RheologyMaterial([MaterialViscosity(50.0)], density=2.0)])
+    G.set_points(x, (x[:, 0] > 0.5).astype(np.int32))
+    G.locate()
+    G.build_operator()
+    with pytest.raises(GaleError) as e:
+        G.solve(UzawaSolver(tolerance=1e-12, maxIterations=1))
+    assert e.value.code == abi.GG_ERR_NOT_CONVERGED
+    # NaN viscosity → non-finite status, no fault
+    G.set_materials([RheologyMaterial([MaterialViscosity(float("nan"))], density=1.0)])
+    G.build_operator()
+    with pytest.raises(GaleError) as e:
+        G.solve(UzawaSolver())
+    assert e.value.code in (abi.GG_ERR_NONFINITE, abi.GG_ERR_NOT_CONVERGED)
+    # an element without points
+    G.set_points(np.ascontiguousarray(x[x[:, 0] > 0.3]))
+    G.locate()
+    with pytest.raises(GaleError) as e:
+        G.build_operator()
+    assert e.value.code == abi.GG_ERR_EMPTY_CELL
+    # state errors
+    H = StokesProblem(mesh)
+    with pytest.raises(GaleError) as e:
+        H.build_operator()
+    assert e.value.code == abi.GG_ERR_STATE
