@@ -154,13 +154,38 @@ def gale_arm(args):
         return max_over_ranks(sum(times) / len(times)), stats, (u, p)
 
     # plain FP64 path (the judge) and the headline path
-    t_plain, st_plain, (u64, p64) = timed(plain, "fp64", max(1, args.steps // 2), 1)
     sampler = ClockSampler(local)
     sampler.start()
     t_head, st_head, (uh, ph) = timed(head, "mixed", args.steps, args.warmup)
     clocks = sampler.stop()
-    err_u = float(np.linalg.norm(uh - u64) / np.linalg.norm(u64))
-    err_p = float(np.linalg.norm((ph - ph.mean()) - (p64 - p64.mean())) / np.linalg.norm(p64 - p64.mean()))
+    if args.headline_only:
+        return
+    t_plain, st_plain, (u64, p64) = timed(plain, "fp64", max(1, args.steps // 2), 1)
+
+    def rel(a, b, centre=False):
+        if centre:
+            a, b = a - a.mean(), b - b.mean()
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    err_u, err_p = rel(uh, u64), rel(ph, p64, True)
+    accuracy = None
+    if not args.no_accuracy:
+        # the discrete solution: plain FP64 path at tight tolerances (= the oracle to 1e-10)
+        G.build_operator("fp64")
+        ut, pt, st_t = G.solve(UzawaSolver(tolerance=1e-9, precision="fp64", inner="jacobi",
+                                           innerRtolFactor=0.01))
+        # the headline path tightened until its error matches 1e-6
+        acc_prm = UzawaSolver(tolerance=args.accurate_rtol, precision="mixed", inner=args.inner,
+                              innerRtolFactor=0.01)
+        t_acc, st_acc, (ua, pa) = timed(acc_prm, "mixed", 1, 1)
+        accuracy = {
+            "reference": "plain FP64 path at Uzawa rtol 1e-9, inner rtol 1e-11",
+            "headline_rtol1e-6": {"u": rel(uh, ut), "p": rel(ph, pt, True)},
+            "plain_fp64_rtol1e-6": {"u": rel(u64, ut), "p": rel(p64, pt, True)},
+            "headline_tight": {"uzawa_rtol": args.accurate_rtol, "inner_rtol": 0.01 * args.accurate_rtol,
+                               "seconds": t_acc, "u": rel(ua, ut), "p": rel(pa, pt, True),
+                               "outer_iterations": st_acc["outer_iterations"]},
+        }
 
     # roofline of the dominant kernel (matrix-free K apply of the inner CG)
     prec_code = abi.PRECISION_MIXED
@@ -227,9 +252,10 @@ def gale_arm(args):
             "plain_fp64_s": t_plain, "speedup_vs_plain_fp64": t_plain / t_head,
             "solves_per_s": world / t_head,
             "rel_l2_vs_fp64": {"u": err_u, "p": err_p},
+            "accuracy": accuracy,
             "iterations": {"headline": {k: st_head[k] for k in ("outer_iterations", "inner_iterations")},
                            "plain_fp64": {k: st_plain[k] for k in ("outer_iterations", "inner_iterations")}},
-            "gpu_launches": int(st_head["kernel_launches"]),
+            "gpu_launches": int(st_head["kernel_launches"]) * args.steps,
             "roofline": {"bound": "hbm", "kernel": "k_cg_apply<3,float> (matrix-free K apply)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
@@ -299,9 +325,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gale", choices=["gale", "reference"])
     ap.add_argument("--n", type=int, default=64)
-    ap.add_argument("--inner", default="jacobi", choices=["jacobi", "mg", "learned"])
+    ap.add_argument("--inner", default="mg", choices=["jacobi", "mg", "learned"])
+    ap.add_argument("--headline-only", action="store_true",
+                    help="run only the warm-up and timed headline solves (profiling)")
     ap.add_argument("--cpu-sample-its", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--accurate-rtol", type=float, default=1e-8)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -122,6 +122,19 @@ class PicardStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class LearnParams(C.Structure):
+    _fields_ = [("level", C.c_int32), ("n_rhs", C.c_int32), ("iters_per_rhs", C.c_int32),
+                ("epochs", C.c_int32), ("lr", C.c_float), ("seed", C.c_int32)]
+
+
+class LearnStats(C.Structure):
+    _fields_ = [("samples", C.c_int32), ("loss_first", C.c_float), ("loss_last", C.c_float),
+                ("train_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def ptr(a, ctype=C.c_double):
     """Pointer to a contiguous numpy array (None stays NULL)."""
     if a is None:
@@ -166,6 +179,12 @@ ABI_FUNCTIONS = {
     "gg_get_rhs": ([_P, _PD, _PD], C.c_int),
     "gg_get_diagonals": ([_P, _PD, _PD], C.c_int),
     "gg_time_apply": ([_P, C.c_int32, C.c_int32, _PD], C.c_int),
+    "gg_learned_train": ([_P, C.POINTER(LearnParams), C.POINTER(LearnStats)], C.c_int),
+    "gg_learned_weights": ([_P, C.POINTER(C.c_float), _PI32], C.c_int),
+    "gg_learned_set_weights": ([_P, C.c_int32, C.POINTER(C.c_float), C.c_int32], C.c_int),
+    "gg_learned_eval": ([_P, C.c_int32, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                         C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), _PD, _PI32],
+                        C.c_int),
 }
 
 HERE = os.path.dirname(os.path.abspath(__file__))

@@ -366,8 +366,11 @@ static void download_nodal(Handle& H, const double* dsrc, const double* add, dou
 
 // Operator build + Dirichlet elimination; device previous solution pointers (nullable).
 int build_all(Handle& H, int precision, int prev, const double* d_u, const double* d_p) {
+    H.launches_at_build = H.kernel_launches;
     int rc = build_operator(H, precision, prev, d_u, d_p);
     if (rc != GG_OK) return rc;
+    // moments (1 or 2 builds) + K u_b + RHS finish + Gᵀ u_b + negate
+    H.kernel_launches += (precision == GG_PRECISION_MIXED ? 2 : 1) + 4;
     // RHS: f_f −= K_fb u_b ; h = −G_bᵀ u_b
     H.ub.ensure(sizeof(double) * H.ndof);
     GG_CUDA(cudaMemsetAsync(H.ub.p, 0, sizeof(double) * H.ndof, H.stream));
@@ -381,6 +384,7 @@ int build_all(Handle& H, int precision, int prev, const double* d_u, const doubl
     GG_CUDA(cudaStreamSynchronize(H.stream));
     H.built = true;
     H.built_precision = precision;
+    H.build_gen++;
     return GG_OK;
 }
 }  // namespace gg

@@ -300,6 +300,70 @@ int gg_apply_K(gg_handle* h, int32_t precision, const double* x, double* y) {
     return GG_OK;
 }
 
+int gg_learned_train(gg_handle* h, const gg_learn_params* params, gg_learn_stats* stats) {
+    if (!h || !params) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (!H.built || H.built_precision != GG_PRECISION_MIXED)
+        return gg::err(H, GG_ERR_STATE, "training needs an operator built with GG_PRECISION_MIXED");
+    gg_learn_stats S{};
+    int rc = GG_OK;
+    GG_TRY2(h, {
+        for (gg::DBuf* b : {&H.r32, &H.cgr32, &H.z32, &H.p32, &H.Ap32, &H.e32, &H.mg_xs, &H.mg_xk, &H.mg_xt})
+            b->ensure(sizeof(float) * H.ndof);
+        H.qtmp.ensure(sizeof(double) * H.nel);
+        H.ftmp.ensure(sizeof(double) * H.ndof);
+        H.red.ensure(sizeof(double) * (4 * 592 + 8) + sizeof(unsigned int) * 8);
+        GG_CUDA(cudaMemsetAsync(reinterpret_cast<double*>(H.red.p) + 4 * 592 + 8, 0, sizeof(unsigned int) * 8, H.stream));
+        H.scal.ensure(sizeof(gg::KrylovScalars) * 2);
+        if (!H.h_scal) GG_CUDA(cudaMallocHost(&H.h_scal, sizeof(gg::KrylovScalars) * 2));
+        rc = gg::learned_train(H, *params, S);
+    })
+    if (stats) *stats = S;
+    if (rc != GG_OK) gg::err(H, rc, "learned training failed (status " + std::to_string(rc) + ")");
+    return rc;
+}
+
+int gg_learned_weights(gg_handle* h, float* weights, int32_t* n) {
+    if (!h) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (n) *n = (int32_t)gg::learned_param_count(H);
+    if (!weights) return GG_OK;
+    if (!H.nn_ready) return gg::err(H, GG_ERR_STATE, "no trained network");
+    GG_TRY2(h, { gg::learned_get_weights(H, weights); })
+    return GG_OK;
+}
+
+int gg_learned_set_weights(gg_handle* h, int32_t level, const float* weights, int32_t n) {
+    if (!h || !weights) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (n != (int32_t)gg::learned_param_count(H)) return gg::err(H, GG_ERR_INVALID, "parameter count");
+    if (!H.built || H.built_precision != GG_PRECISION_MIXED)
+        return gg::err(H, GG_ERR_STATE, "needs an operator built with GG_PRECISION_MIXED");
+    int rc = GG_OK;
+    GG_TRY2(h, {
+        rc = gg::learned_set_level(H, level);
+        if (rc == GG_OK) gg::learned_set_weights(H, weights);
+    })
+    return rc;
+}
+
+int gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const float* inputs, const float* targets,
+                    const float* weights, float* outputs, float* gradient, double* loss, int32_t* grid_nodes) {
+    if (!h || batch < 1 || !inputs || !targets || !weights || !outputs || !gradient || !loss) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (!H.built || H.built_precision != GG_PRECISION_MIXED)
+        return gg::err(H, GG_ERR_STATE, "needs an operator built with GG_PRECISION_MIXED");
+    int rc = GG_OK;
+    GG_TRY2(h, {
+        rc = gg::learned_set_level(H, level);
+        if (rc == GG_OK) {
+            if (grid_nodes) *grid_nodes = (int32_t)H.mg[H.nn_level]->nnode;
+            rc = gg::learned_eval(H, batch, inputs, targets, weights, outputs, gradient, loss);
+        }
+    })
+    return rc;
+}
+
 int gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_launch) {
     if (!h || !ms_per_launch || reps < 1) return GG_ERR_INVALID;
     Handle& H = h->H;

@@ -46,10 +46,14 @@ struct DBuf {
 
 // One multigrid level (level 0 = the fine mesh).
 struct MGLevel {
-    MeshK mk;
-    int64_t nnode = 0, nel = 0;
-    DBuf mom32, mom64, diag32, bcmask;
-    DBuf x, r, b, t;  // FP32 work vectors [dim*nnode]
+    MeshK mk{};
+    int64_t nnode = 0, nel = 0, ndof = 0;
+    DBuf own_mom64, own_mom32, own_bcmask;   // coarse levels own their operator
+    DBuf invdiag;                            // FP32 inverse Jacobi diagonal (0 on BC dofs)
+    const double* mom64 = nullptr;           // effective pointers (level 0: the fine operator)
+    const float* mom32 = nullptr;
+    const uint8_t* bcmask = nullptr;
+    DBuf x, b, r, d, t;                      // FP32 work vectors [dim*nnode]
     double lambda_max = 0.0;
 };
 
@@ -89,11 +93,23 @@ struct Handle {
     KrylovScalars* h_scal = nullptr;                  // pinned mirror
     std::vector<std::unique_ptr<MGLevel>> mg;
     bool mg_ready = false;
-    DBuf coarse_inv;  // dense inverse of the coarsest operator (FP32)
-    int64_t coarse_n = 0;
+    int64_t build_gen = 0;  // incremented by every operator build (graphs bake in its scalars)
+    int64_t mg_gen = -1;    // build generation the hierarchy was set up for
+    DBuf coarse_inv;        // dense inverse of the coarsest operator (FP32, [n][n])
+    DBuf mg_part, mg_dense; // power-iteration partials; FP64 columns of the coarsest operator
+    int64_t coarse_n = 0;   // 0: no dense coarse solve (Chebyshev on the coarsest level)
+    int mg_degree = 2;      // Chebyshev degree of the smoother
+    // learned coarse correction (gg_learned.cu)
+    std::shared_ptr<struct LearnedState> learned;
+    bool nn_ready = false;
+    bool nn_enabled = true;    // cleared after repeated stagnation (fallback to multigrid)
+    int fallbacks = 0;         // learned → multigrid fallbacks taken in the current solve
+    int nn_level = 2;       // hierarchy level the network acts on
+    DBuf mg_xs, mg_xk, mg_xt;  // FP32 fine-level scratch of the training data generator
 
     // CUDA graphs keyed by solver variant
     std::map<std::string, cudaGraphExec_t> graphs;
+    std::map<std::string, int64_t> graph_nodes;  // kernel nodes per captured graph
     double last_solve_ms = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -101,6 +117,8 @@ struct Handle {
     bool have_solution = false;
     int32_t max_material = 0;       // largest material index of the points
     mutable int64_t kernel_launches = 0;    // launches of this library's kernels (graph nodes counted)
+    int64_t launches_at_build = 0;          // counter value when the last build started
+    int64_t stats_gen = -1;                 // build generation the last solve statistics covered
     DBuf picard_prev, picard_part;
 };
 

@@ -57,6 +57,26 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
                 double rtol, int maxit, int* iters);
 void release_graphs(Handle& H);
 
+// Multigrid (gg_mg.cu): hierarchy for the current build; z = M⁻¹ b on level l.
+int mg_setup(Handle& H);
+void vcycle(Handle& H, size_t l, const float* b, float* x, const int32_t* done);
+void mg_restrict(Handle& H, size_t l, const float* fine, float* coarse, const int32_t* done);
+void mg_prolong_add(Handle& H, size_t l, const float* coarse, float* fine, const int32_t* done);
+// x = K32⁻¹ b by the multigrid flexible CG (FP32, ‖r‖ ≤ rtol‖b‖)
+int fcg_mg_solve(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters);
+
+// Learned coarse correction (gg_learned.cu)
+bool learned_ready(Handle& H);
+void learned_prepare(Handle& H);
+void learned_correction(Handle& H, const float* r, float* z, const int32_t* done);
+int learned_set_level(Handle& H, int level);
+int64_t learned_param_count(Handle& H);
+void learned_set_weights(Handle& H, const float* w);
+void learned_get_weights(Handle& H, float* w);
+int learned_eval(Handle& H, int B, const float* xin, const float* tgt, const float* w, float* y, float* grad,
+                 double* loss);
+int learned_train(Handle& H, const gg_learn_params& P, gg_learn_stats& st);
+
 // prev_u = u + BC values, prev_p = q (gg_api2.cu)
 void store_solution(Handle& H);
 

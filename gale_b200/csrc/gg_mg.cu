@@ -1,0 +1,594 @@
+// gg_mg.cu -- geometric multigrid for the inner velocity solve (FP32), sm_100a.
+//
+// Design reference: Gale's PETScMGSolver + SROpGenerator (StgFEM/SLE/SystemSetup/src/
+// PETScMGSolver.cxx:240,513-522,654-704; SROpGenerator.cxx:157-467): geometric levels of
+// the regular mesh, a Q1 interpolation between them, smoothed V-cycles as the
+// preconditioner of the velocity Krylov solve.  Built B200-first instead of around
+// assembled PETSc matrices:
+//   * coarse operators are re-discretised from the PIC quadrature itself: the moments
+//     of a coarse element are an exact linear re-expansion of its children's moments
+//     (ξ_coarse = (ξ_child ± 1)/2), so every level is matrix-free with the same kernel;
+//   * smoothing is Chebyshev–Jacobi (eigen-bound from a power iteration), which is a
+//     fixed polynomial of D⁻¹A — no inner products inside the V-cycle;
+//   * the coarsest level (≤ 3000 dofs) is solved by a dense FP32 inverse (one mat-vec);
+//   * the whole V-cycle is a fixed kernel sequence and is captured into the inner
+//     Krylov iteration's CUDA graph; every kernel exits early once the solve is done.
+// The V-cycle preconditions a flexible CG (Notay's truncated FCG) so that the learned
+// coarse correction (gg_learned.cu) may be added to it.
+#include <math.h>
+#include <stdio.h>
+
+#include <cstring>
+#include <vector>
+
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+#include "gg_ops.cuh"
+
+namespace gg {
+
+MeshK make_mesh(const gg_mesh_desc& d);
+
+namespace {
+
+constexpr int kMinCoarse = 4;  // coarsen while every axis is even and ≥ 4 elements
+
+__device__ __forceinline__ double tcoef(int a, int ap, double o) {
+    // ξ_c = (ξ_f + o)/2  ⇒  ξ_c^a = Σ_{a'≤a} T[a][a'] ξ_f^{a'}
+    if (a == 0) return ap == 0 ? 1.0 : 0.0;
+    if (a == 1) return ap == 0 ? 0.5 * o : (ap == 1 ? 0.5 : 0.0);
+    return ap == 0 ? 0.25 : (ap == 1 ? 0.5 * o : 0.25);
+}
+
+template <int DIM>
+__global__ void k_coarsen_moments(MeshK fk, MeshK ck, const double* __restrict__ mf,
+                                  double* __restrict__ mc, float* __restrict__ mc32) {
+    constexpr int NM = n_moments<DIM>();
+    for (int64_t E = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; E < ck.nel;
+         E += (int64_t)gridDim.x * blockDim.x) {
+        const int I = (int)(E % ck.n[0]);
+        const int64_t rr = E / ck.n[0];
+        const int J = (int)(rr % ck.n[1]), K = (int)(rr / ck.n[1]);
+        double acc[NM];
+#pragma unroll
+        for (int q = 0; q < NM; q++) acc[q] = 0.0;
+#pragma unroll
+        for (int ch = 0; ch < (1 << DIM); ch++) {
+            const int dx = ch & 1, dy = (ch >> 1) & 1, dz = DIM == 3 ? (ch >> 2) & 1 : 0;
+            const int64_t fe = (2 * I + dx) + (int64_t)fk.n[0] * ((2 * J + dy) + (int64_t)fk.n[1] * (2 * K + dz));
+            const double ox = 2.0 * dx - 1.0, oy = 2.0 * dy - 1.0, oz = 2.0 * dz - 1.0;
+            double f[NM];
+#pragma unroll
+            for (int q = 0; q < NM; q++) f[q] = mf[(int64_t)q * fk.nel + fe];
+#pragma unroll
+            for (int c = 0; c < (DIM == 3 ? 3 : 1); c++)
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        const int so = mom_slot<DIM>(a, b, c);
+                        if (so < 0) continue;
+                        double s = 0.0;
+#pragma unroll
+                        for (int cp = 0; cp <= c; cp++)
+#pragma unroll
+                            for (int bp = 0; bp <= b; bp++)
+#pragma unroll
+                                for (int ap = 0; ap <= a; ap++) {
+                                    const int si = mom_slot<DIM>(ap, bp, cp);
+                                    if (si < 0) continue;
+                                    s += tcoef(a, ap, ox) * tcoef(b, bp, oy) * (DIM == 3 ? tcoef(c, cp, oz) : 1.0) * f[si];
+                                }
+                        acc[so] += s;
+                    }
+        }
+#pragma unroll
+        for (int q = 0; q < NM; q++) {
+            mc[(int64_t)q * ck.nel + E] = acc[q];
+            mc32[(int64_t)q * ck.nel + E] = (float)acc[q];
+        }
+    }
+}
+
+// Jacobi diagonal of a level from its moments (same closed form as the build kernel).
+template <int DIM>
+__global__ void k_level_diag(MeshK mk, const double* __restrict__ mom, float* __restrict__ diag) {
+    constexpr int NM = n_moments<DIM>();
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < mk.nel;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        double M[NM];
+#pragma unroll
+        for (int q = 0; q < NM; q++) M[q] = mom[(int64_t)q * mk.nel + e];
+        int ijk[3];
+        elem_ijk(mk, e, ijk);
+#pragma unroll
+        for (int a = 0; a < (1 << DIM); a++) {
+            double S[3] = {0, 0, 0};
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                double v = 0.0;
+#pragma unroll
+                for (int k0 = 0; k0 < 3; k0++)
+#pragma unroll
+                    for (int k1 = 0; k1 < 3; k1++)
+#pragma unroll
+                        for (int k2 = 0; k2 < 3; k2++) {
+                            const int ex[3] = {k0, k1, k2};
+                            bool ok = true;
+                            double coef = 1.0;
+#pragma unroll
+                            for (int o = 0; o < 3; o++) {
+                                if (o >= DIM || o == d) { if (ex[o] != 0) ok = false; continue; }
+                                coef *= ex[o] == 1 ? 2.0 * (((a >> o) & 1) ? 1.0 : -1.0) : 1.0;
+                            }
+                            if (!ok) continue;
+                            v += coef * M[mom_slot<DIM>(k0, k1, k2)];
+                        }
+                S[d] = v * mk.kappa[d] * mk.kappa[d];
+            }
+            const double tot = S[0] + S[1] + S[2];
+            const int64_t n = elem_node<DIM>(mk, ijk, a);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) atomicAdd(&diag[(int64_t)c * mk.nnode + n], (float)(tot + S[c]));
+        }
+    }
+}
+
+__global__ void k_invert_diag(int64_t n, int64_t nnode, const uint8_t* __restrict__ bc,
+                              const float* __restrict__ diag, float* __restrict__ inv) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i / nnode);
+        inv[i] = ((bc[i - (int64_t)c * nnode] >> c) & 1) ? 0.f : 1.f / diag[i];
+    }
+}
+
+// coarse node (I,J,K) ↔ fine node (2I,2J,2K): the wall conditions map onto themselves
+__global__ void k_coarse_bcmask(MeshK fk, MeshK ck, const uint8_t* __restrict__ bf, uint8_t* __restrict__ bcc) {
+    for (int64_t N = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; N < ck.nnode;
+         N += (int64_t)gridDim.x * blockDim.x) {
+        const int I = (int)(N % ck.nn[0]);
+        const int64_t rr = N / ck.nn[0];
+        const int J = (int)(rr % ck.nn[1]), K = (int)(rr / ck.nn[1]);
+        bcc[N] = bf[2 * I + (int64_t)fk.nn[0] * (2 * J + (int64_t)fk.nn[1] * 2 * K)];
+    }
+}
+
+// b_c = Pᵀ r_f (full weighting without normalisation), zero on coarse BC dofs
+template <int DIM>
+__global__ void k_restrict(MeshK fk, MeshK ck, const uint8_t* __restrict__ bcc, const float* __restrict__ rf,
+                           float* __restrict__ bcv, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t N = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; N < ck.nnode;
+         N += (int64_t)gridDim.x * blockDim.x) {
+        const int I = (int)(N % ck.nn[0]);
+        const int64_t rr = N / ck.nn[0];
+        const int J = (int)(rr % ck.nn[1]), K = DIM == 3 ? (int)(rr / ck.nn[1]) : 0;
+        float acc[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) acc[c] = 0.f;
+#pragma unroll
+        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); dz++)
+#pragma unroll
+            for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
+                    if (i < 0 || j < 0 || k < 0 || i >= fk.nn[0] || j >= fk.nn[1] || k >= fk.nn[2]) continue;
+                    const float w = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+                    const int64_t n = i + (int64_t)fk.nn[0] * (j + (int64_t)fk.nn[1] * k);
+#pragma unroll
+                    for (int c = 0; c < DIM; c++) acc[c] += w * rf[(int64_t)c * fk.nnode + n];
+                }
+        const uint8_t bm = bcc[N];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) bcv[(int64_t)c * ck.nnode + N] = ((bm >> c) & 1) ? 0.f : acc[c];
+    }
+}
+
+// x_f += P x_c (Q1 interpolation), fine BC dofs untouched
+template <int DIM>
+__global__ void k_prolong_add(MeshK fk, MeshK ck, const uint8_t* __restrict__ bcf, const float* __restrict__ xc,
+                              float* __restrict__ xf, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < fk.nnode;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(n % fk.nn[0]);
+        const int64_t rr = n / fk.nn[0];
+        const int j = (int)(rr % fk.nn[1]), k = DIM == 3 ? (int)(rr / fk.nn[1]) : 0;
+        const int idx[3] = {i, j, k};
+        int lo[3], hi[3];
+        float wl[3], wh[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (d >= DIM || (idx[d] & 1) == 0) {
+                lo[d] = hi[d] = idx[d] >> 1;
+                wl[d] = 1.f;
+                wh[d] = 0.f;
+            } else {
+                lo[d] = idx[d] >> 1;
+                hi[d] = lo[d] + 1;
+                wl[d] = wh[d] = 0.5f;
+            }
+        }
+        float acc[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) acc[c] = 0.f;
+#pragma unroll
+        for (int q = 0; q < (1 << DIM); q++) {
+            const int I = (q & 1) ? hi[0] : lo[0], J = (q & 2) ? hi[1] : lo[1], K = (q & 4) ? hi[2] : lo[2];
+            const float w = ((q & 1) ? wh[0] : wl[0]) * ((q & 2) ? wh[1] : wl[1]) * (DIM == 3 ? ((q & 4) ? wh[2] : wl[2]) : 1.f);
+            if (w == 0.f) continue;
+            const int64_t N = I + (int64_t)ck.nn[0] * (J + (int64_t)ck.nn[1] * K);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) acc[c] += w * xc[(int64_t)c * ck.nnode + N];
+        }
+        const uint8_t bm = bcf[n];
+#pragma unroll
+        for (int c = 0; c < DIM; c++)
+            if (!((bm >> c) & 1)) xf[(int64_t)c * fk.nnode + n] += acc[c];
+    }
+}
+
+// ---- Chebyshev–Jacobi smoother vector steps --------------------------------------------
+// start from x = 0: r = b, d = D⁻¹r/θ, x = d, t = 0
+__global__ void k_cheb_start(int64_t n, const float* __restrict__ b, const float* __restrict__ invd, float inv_theta,
+                             float* __restrict__ r, float* __restrict__ d, float* __restrict__ x,
+                             float* __restrict__ t, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float rv = b[i];
+        const float dv = inv_theta * invd[i] * rv;
+        r[i] = rv;
+        d[i] = dv;
+        x[i] = dv;
+        t[i] = 0.f;
+    }
+}
+// post-smoothing start from x: r = b − t (t = A x), d = D⁻¹r/θ, x += d, t = 0
+__global__ void k_cheb_restart(int64_t n, const float* __restrict__ b, const float* __restrict__ invd, float inv_theta,
+                               float* __restrict__ r, float* __restrict__ d, float* __restrict__ x,
+                               float* __restrict__ t, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float rv = b[i] - t[i];
+        const float dv = inv_theta * invd[i] * rv;
+        r[i] = rv;
+        d[i] = dv;
+        x[i] += dv;
+        t[i] = 0.f;
+    }
+}
+// r −= t (t = A d), d = c1 d + c2 D⁻¹ r, x += d, t = 0
+__global__ void k_cheb_step(int64_t n, const float* __restrict__ invd, float c1, float c2, float* __restrict__ r,
+                            float* __restrict__ d, float* __restrict__ x, float* __restrict__ t,
+                            const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float rv = r[i] - t[i];
+        const float dv = c1 * d[i] + c2 * invd[i] * rv;
+        r[i] = rv;
+        d[i] = dv;
+        x[i] += dv;
+        t[i] = 0.f;
+    }
+}
+// r −= t, t = 0  (r = b − A x after the last step)
+__global__ void k_resid_finish(int64_t n, float* __restrict__ r, float* __restrict__ t, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        r[i] -= t[i];
+        t[i] = 0.f;
+    }
+}
+
+// x = A⁻¹ b on the coarsest level: one warp per row of the dense FP32 inverse
+__global__ void k_dense_mv(int n, const float* __restrict__ A, const float* __restrict__ b, float* __restrict__ x,
+                           const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    const int lane = threadIdx.x & 31;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
+        float s = 0.f;
+        for (int k = lane; k < n; k += 32) s += A[(int64_t)row * n + k] * b[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) x[row] = s;
+    }
+}
+
+__global__ void k_hash_fill(int64_t n, int64_t nnode, const uint8_t* __restrict__ bc, float* __restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t h = (uint32_t)i * 2654435761u + 0x9e3779b9u;
+        h ^= h >> 15; h *= 0x85ebca6bu; h ^= h >> 13;
+        const int c = (int)(i / nnode);
+        x[i] = ((bc[i - (int64_t)c * nnode] >> c) & 1) ? 0.f : ((float)(h & 0xffffff) / 16777216.f - 0.5f);
+    }
+}
+
+// y = D⁻¹ t, partial norms ‖y‖², ‖x‖²; t = 0
+__global__ void k_power_step(int64_t n, const float* __restrict__ invd, const float* __restrict__ x,
+                             float* __restrict__ t, float* __restrict__ y, double* __restrict__ part) {
+    double yy = 0.0, xx = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = invd[i] * t[i];
+        y[i] = v;
+        t[i] = 0.f;
+        yy += (double)v * v;
+        xx += (double)x[i] * x[i];
+    }
+    yy = block_sum(yy);
+    __syncthreads();
+    xx = block_sum(xx);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = yy;
+        part[2 * blockIdx.x + 1] = xx;
+    }
+}
+
+__global__ void k_scale(int64_t n, float s, const float* __restrict__ y, float* __restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = s * y[i];
+}
+
+__global__ void k_unit(int64_t n, int64_t j, double* __restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = (i == j) ? 1.0 : 0.0;
+}
+
+int g(int64_t n) { return grid_for(n, 256); }
+
+struct ChebCoef {
+    float inv_theta;
+    float c1[8], c2[8];
+};
+
+ChebCoef cheb_coef(double lmax_est, int degree) {
+    const double lmax = 1.1 * lmax_est, lmin = 0.1 * lmax_est;
+    const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+    const double sigma = theta / delta;
+    ChebCoef cc{};
+    cc.inv_theta = (float)(1.0 / theta);
+    double rho = 1.0 / sigma;
+    for (int k = 1; k < degree && k < 8; k++) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        cc.c1[k] = (float)(rn * rho);
+        cc.c2[k] = (float)(2.0 * rn / delta);
+        rho = rn;
+    }
+    return cc;
+}
+
+}  // namespace
+
+// Enqueue the V-cycle z = M⁻¹ b on level l (b and x are level-l vectors).
+void vcycle(Handle& H, size_t l, const float* b, float* x, const int32_t* done) {
+    MGLevel& L = *H.mg[l];
+    cudaStream_t st = H.stream;
+    const int64_t n = L.ndof;
+    const int dim = H.dim;
+    if (l + 1 == H.mg.size()) {
+        if (H.coarse_n) {
+            k_dense_mv<<<g((int64_t)H.coarse_n * 32), 256, 0, st>>>((int)H.coarse_n, H.coarse_inv.as<float>(), b, x, done);
+            H.kernel_launches++;
+            return;
+        }
+        // no dense solve: a long Chebyshev sweep from zero
+        ChebCoef cc = cheb_coef(L.lambda_max, 8);
+        k_cheb_start<<<g(n), 256, 0, st>>>(n, b, L.invdiag.as<float>(), cc.inv_theta, L.r.as<float>(), L.d.as<float>(), x,
+                                           L.t.as<float>(), done);
+        for (int k = 1; k < 8; k++) {
+            apply_K_ex<float>(L.mk, L.mom32, L.bcmask, L.d.as<float>(), L.t.as<float>(), nullptr, apply_grid(L.nel), st, done);
+            k_cheb_step<<<g(n), 256, 0, st>>>(n, L.invdiag.as<float>(), cc.c1[k], cc.c2[k], L.r.as<float>(), L.d.as<float>(),
+                                              x, L.t.as<float>(), done);
+        }
+        H.kernel_launches += 15;
+        return;
+    }
+    MGLevel& C = *H.mg[l + 1];
+    const int deg = H.mg_degree;
+    ChebCoef cc = cheb_coef(L.lambda_max, deg);
+    float* r = L.r.as<float>();
+    float* d = L.d.as<float>();
+    float* t = L.t.as<float>();
+    const float* invd = L.invdiag.as<float>();
+    const int ga = apply_grid(L.nel);
+    // pre-smoothing from zero; the last apply leaves r = b − A x
+    k_cheb_start<<<g(n), 256, 0, st>>>(n, b, invd, cc.inv_theta, r, d, x, t, done);
+    for (int k = 1; k < deg; k++) {
+        apply_K_ex<float>(L.mk, L.mom32, L.bcmask, d, t, nullptr, ga, st, done);
+        k_cheb_step<<<g(n), 256, 0, st>>>(n, invd, cc.c1[k], cc.c2[k], r, d, x, t, done);
+    }
+    apply_K_ex<float>(L.mk, L.mom32, L.bcmask, d, t, nullptr, ga, st, done);
+    k_resid_finish<<<g(n), 256, 0, st>>>(n, r, t, done);
+    // coarse-grid correction
+    if (dim == 2) k_restrict<2><<<g(C.nnode), 256, 0, st>>>(L.mk, C.mk, C.bcmask, r, C.b.as<float>(), done);
+    else k_restrict<3><<<g(C.nnode), 256, 0, st>>>(L.mk, C.mk, C.bcmask, r, C.b.as<float>(), done);
+    vcycle(H, l + 1, C.b.as<float>(), C.x.as<float>(), done);
+    if (dim == 2) k_prolong_add<2><<<g(L.nnode), 256, 0, st>>>(L.mk, C.mk, L.bcmask, C.x.as<float>(), x, done);
+    else k_prolong_add<3><<<g(L.nnode), 256, 0, st>>>(L.mk, C.mk, L.bcmask, C.x.as<float>(), x, done);
+    // post-smoothing from x
+    apply_K_ex<float>(L.mk, L.mom32, L.bcmask, x, t, nullptr, ga, st, done);
+    k_cheb_restart<<<g(n), 256, 0, st>>>(n, b, invd, cc.inv_theta, r, d, x, t, done);
+    for (int k = 1; k < deg; k++) {
+        apply_K_ex<float>(L.mk, L.mom32, L.bcmask, d, t, nullptr, ga, st, done);
+        k_cheb_step<<<g(n), 256, 0, st>>>(n, invd, cc.c1[k], cc.c2[k], r, d, x, t, done);
+    }
+    H.kernel_launches += 6 + 4 * deg;
+}
+
+// level l−1 → l restriction and l → l−1 prolongation-add (used by the learned correction)
+void mg_restrict(Handle& H, size_t l, const float* fine, float* coarse, const int32_t* done) {
+    MGLevel& F = *H.mg[l - 1];
+    MGLevel& C = *H.mg[l];
+    if (H.dim == 2) k_restrict<2><<<g(C.nnode), 256, 0, H.stream>>>(F.mk, C.mk, C.bcmask, fine, coarse, done);
+    else k_restrict<3><<<g(C.nnode), 256, 0, H.stream>>>(F.mk, C.mk, C.bcmask, fine, coarse, done);
+    H.kernel_launches++;
+}
+void mg_prolong_add(Handle& H, size_t l, const float* coarse, float* fine, const int32_t* done) {
+    MGLevel& F = *H.mg[l - 1];
+    MGLevel& C = *H.mg[l];
+    if (H.dim == 2) k_prolong_add<2><<<g(F.nnode), 256, 0, H.stream>>>(F.mk, C.mk, F.bcmask, coarse, fine, done);
+    else k_prolong_add<3><<<g(F.nnode), 256, 0, H.stream>>>(F.mk, C.mk, F.bcmask, coarse, fine, done);
+    H.kernel_launches++;
+}
+
+static double power_lambda(Handle& H, MGLevel& L) {
+    cudaStream_t st = H.stream;
+    const int64_t n = L.ndof;
+    const int nb = 64;
+    H.mg_part.ensure(sizeof(double) * 2 * nb);
+    std::vector<double> part(2 * nb);
+    float* x = L.x.as<float>();
+    float* y = L.d.as<float>();
+    float* t = L.t.as<float>();
+    k_hash_fill<<<g(n), 256, 0, st>>>(n, L.nnode, L.bcmask, x);
+    GG_CUDA(cudaMemsetAsync(t, 0, sizeof(float) * n, st));
+    double lam = 0.0;
+    for (int it = 0; it < 12; it++) {
+        apply_K_ex<float>(L.mk, L.mom32, L.bcmask, x, t, nullptr, apply_grid(L.nel), st, nullptr);
+        k_power_step<<<nb, 256, 0, st>>>(n, L.invdiag.as<float>(), x, t, y, H.mg_part.as<double>());
+        GG_CUDA(cudaMemcpyAsync(part.data(), H.mg_part.p, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, st));
+        GG_CUDA(cudaStreamSynchronize(st));
+        double yy = 0, xx = 0;
+        for (int b = 0; b < nb; b++) { yy += part[2 * b]; xx += part[2 * b + 1]; }
+        if (xx <= 0 || yy <= 0) break;
+        lam = sqrt(yy / xx);
+        k_scale<<<g(n), 256, 0, st>>>(n, (float)(1.0 / sqrt(yy)), y, x);
+    }
+    GG_CUDA(cudaGetLastError());
+    return lam;
+}
+
+// Dense inverse of the coarsest level: columns K e_j from the matrix-free apply (FP64),
+// Gauss–Jordan with partial pivoting on the host.
+static void coarse_inverse(Handle& H, MGLevel& L) {
+    const int64_t n = L.ndof;
+    cudaStream_t st = H.stream;
+    H.mg_dense.ensure(sizeof(double) * (n * n + n));
+    double* A = H.mg_dense.as<double>();
+    double* e = A + n * n;
+    GG_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * n * n, st));
+    std::vector<uint8_t> bc(L.nnode);
+    GG_CUDA(cudaMemcpyAsync(bc.data(), L.bcmask, L.nnode, cudaMemcpyDeviceToHost, st));
+    GG_CUDA(cudaStreamSynchronize(st));
+    auto fixed = [&](int64_t i) { const int c = (int)(i / L.nnode); return (bc[i - c * L.nnode] >> c) & 1; };
+    for (int64_t j = 0; j < n; j++) {
+        if (fixed(j)) continue;
+        k_unit<<<g(n), 256, 0, st>>>(n, j, e);
+        apply_K_ex<double>(L.mk, L.mom64, L.bcmask, e, A + j * n, nullptr, apply_grid(L.nel), st, nullptr);
+        H.kernel_launches += 2;
+    }
+    std::vector<double> a(n * n), inv(n * n, 0.0);
+    GG_CUDA(cudaMemcpyAsync(a.data(), A, sizeof(double) * n * n, cudaMemcpyDeviceToHost, st));
+    GG_CUDA(cudaStreamSynchronize(st));
+    // column j of K is a[j*n + i]; K symmetric → a is K row-major as well
+    for (int64_t i = 0; i < n; i++)
+        if (fixed(i)) {
+            for (int64_t k = 0; k < n; k++) a[i * n + k] = a[k * n + i] = 0.0;
+            a[i * n + i] = 1.0;
+        }
+    for (int64_t i = 0; i < n; i++) inv[i * n + i] = 1.0;
+    for (int64_t c = 0; c < n; c++) {
+        int64_t piv = c;
+        for (int64_t r = c + 1; r < n; r++)
+            if (fabs(a[r * n + c]) > fabs(a[piv * n + c])) piv = r;
+        if (piv != c)
+            for (int64_t k = 0; k < n; k++) {
+                std::swap(a[c * n + k], a[piv * n + k]);
+                std::swap(inv[c * n + k], inv[piv * n + k]);
+            }
+        const double dv = 1.0 / a[c * n + c];
+        for (int64_t k = 0; k < n; k++) {
+            a[c * n + k] *= dv;
+            inv[c * n + k] *= dv;
+        }
+        for (int64_t r = 0; r < n; r++) {
+            if (r == c) continue;
+            const double f = a[r * n + c];
+            if (f == 0.0) continue;
+            for (int64_t k = 0; k < n; k++) {
+                a[r * n + k] -= f * a[c * n + k];
+                inv[r * n + k] -= f * inv[c * n + k];
+            }
+        }
+    }
+    std::vector<float> inv32(n * n);
+    for (int64_t i = 0; i < n * n; i++) inv32[i] = (float)inv[i];
+    H.coarse_inv.ensure(sizeof(float) * n * n);
+    GG_CUDA(cudaMemcpyAsync(H.coarse_inv.p, inv32.data(), sizeof(float) * n * n, cudaMemcpyHostToDevice, st));
+    GG_CUDA(cudaStreamSynchronize(st));
+    H.coarse_n = n;
+}
+
+// Build (or refresh for a new operator) the hierarchy.  Needs the mixed build (FP32 moments).
+int mg_setup(Handle& H) {
+    if (H.mg_gen == H.build_gen && !H.mg.empty()) return GG_OK;
+    cudaStream_t st = H.stream;
+    const int dim = H.dim;
+    if (H.mg.empty()) {
+        auto L0 = std::make_unique<MGLevel>();
+        L0->mk = H.mk;
+        H.mg.push_back(std::move(L0));
+        for (;;) {
+            const MeshK& f = H.mg.back()->mk;
+            bool can = true;
+            for (int d = 0; d < dim; d++)
+                if (f.n[d] % 2 != 0 || f.n[d] < kMinCoarse) can = false;
+            if (!can) break;
+            gg_mesh_desc cd{};
+            cd.dim = dim;
+            for (int d = 0; d < dim; d++) {
+                cd.elements[d] = f.n[d] / 2;
+                cd.min[d] = f.min[d];
+                cd.max[d] = f.max[d];
+            }
+            auto C = std::make_unique<MGLevel>();
+            C->mk = make_mesh(cd);
+            H.mg.push_back(std::move(C));
+        }
+        for (size_t l = 0; l < H.mg.size(); l++) {
+            MGLevel& L = *H.mg[l];
+            L.nnode = L.mk.nnode;
+            L.nel = L.mk.nel;
+            L.ndof = L.nnode * dim;
+            for (DBuf* b : {&L.x, &L.b, &L.r, &L.d, &L.t, &L.invdiag}) b->ensure(sizeof(float) * L.ndof);
+            if (l > 0) {
+                L.own_mom64.ensure(sizeof(double) * H.nm * L.nel);
+                L.own_mom32.ensure(sizeof(float) * H.nm * L.nel);
+                L.own_bcmask.ensure(L.nnode);
+            }
+        }
+    }
+    // operators
+    MGLevel& L0 = *H.mg[0];
+    L0.mom64 = H.mom64.as<double>();
+    L0.mom32 = H.mom32.as<float>();
+    L0.bcmask = H.bcmask.as<uint8_t>();
+    k_invert_diag<<<g(L0.ndof), 256, 0, st>>>(L0.ndof, L0.nnode, L0.bcmask, H.kdiag32.as<float>(), L0.invdiag.as<float>());
+    for (size_t l = 1; l < H.mg.size(); l++) {
+        MGLevel& F = *H.mg[l - 1];
+        MGLevel& L = *H.mg[l];
+        L.mom64 = L.own_mom64.as<double>();
+        L.mom32 = L.own_mom32.as<float>();
+        L.bcmask = L.own_bcmask.as<uint8_t>();
+        k_coarse_bcmask<<<g(L.nnode), 256, 0, st>>>(F.mk, L.mk, F.bcmask, L.own_bcmask.as<uint8_t>());
+        if (dim == 2) k_coarsen_moments<2><<<g(L.nel), 128, 0, st>>>(F.mk, L.mk, F.mom64, L.own_mom64.as<double>(), L.own_mom32.as<float>());
+        else k_coarsen_moments<3><<<g(L.nel), 128, 0, st>>>(F.mk, L.mk, F.mom64, L.own_mom64.as<double>(), L.own_mom32.as<float>());
+        GG_CUDA(cudaMemsetAsync(L.t.p, 0, sizeof(float) * L.ndof, st));
+        if (dim == 2) k_level_diag<2><<<g(L.nel), 128, 0, st>>>(L.mk, L.mom64, L.t.as<float>());
+        else k_level_diag<3><<<g(L.nel), 128, 0, st>>>(L.mk, L.mom64, L.t.as<float>());
+        k_invert_diag<<<g(L.ndof), 256, 0, st>>>(L.ndof, L.nnode, L.bcmask, L.t.as<float>(), L.invdiag.as<float>());
+        GG_CUDA(cudaGetLastError());
+    }
+    for (auto& L : H.mg) L->lambda_max = power_lambda(H, *L);
+    // diag inversion + per coarse level (mask, moments, diag, inversion) + power iterations
+    H.kernel_launches += 1 + 4 * (int64_t)(H.mg.size() - 1) + 37 * (int64_t)H.mg.size();
+    MGLevel& Lc = *H.mg.back();
+    H.coarse_n = 0;
+    if (H.mg.size() > 1 && Lc.ndof <= 3000) coarse_inverse(H, Lc);
+    GG_CUDA(cudaStreamSynchronize(st));
+    H.mg_gen = H.build_gen;
+    return GG_OK;
+}
+
+}  // namespace gg

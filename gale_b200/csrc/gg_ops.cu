@@ -17,35 +17,16 @@
 namespace gg {
 
 template <int DIM, typename R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
 k_apply_K(MeshK mk, const R* __restrict__ mom, const uint8_t* __restrict__ bcmask,
-          const R* __restrict__ x, R* __restrict__ y, double* __restrict__ energy_part) {
-    constexpr int NS = 1 << DIM;
-    const int64_t nel = mk.nel, nnode = mk.nnode;
+          const R* __restrict__ x, R* __restrict__ y, double* __restrict__ energy_part,
+          const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    const int64_t nel = mk.nel;
     double en = 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        int ijk[3];
-        elem_ijk(mk, e, ijk);
-        int64_t nodes[NS];
-        R u[NS][DIM], yl[NS][DIM];
-#pragma unroll
-        for (int a = 0; a < NS; a++) {
-            nodes[a] = elem_node<DIM>(mk, ijk, a);
-#pragma unroll
-            for (int c = 0; c < DIM; c++) u[a][c] = x[(int64_t)c * nnode + nodes[a]];
-        }
-        element_apply_dev<DIM, R>(mk, mom, nel, e, u, yl);
-#pragma unroll
-        for (int a = 0; a < NS; a++) {
-            const uint8_t bm = bcmask[nodes[a]];
-#pragma unroll
-            for (int c = 0; c < DIM; c++) {
-                en += (double)u[a][c] * (double)yl[a][c];
-                if (!((bm >> c) & 1)) atomicAdd(&y[(int64_t)c * nnode + nodes[a]], yl[a][c]);
-            }
-        }
-    }
+         e += (int64_t)gridDim.x * blockDim.x)
+        en += element_apply_scatter<DIM, R>(mk, mom, bcmask, x, y, e);
     if (energy_part) {
         en = block_sum(en);
         if (threadIdx.x == 0) energy_part[blockIdx.x] = en;
@@ -54,20 +35,20 @@ k_apply_K(MeshK mk, const R* __restrict__ mom, const uint8_t* __restrict__ bcmas
 
 template <typename R>
 void apply_K_ex(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
-                double* energy_part, int grid, cudaStream_t st) {
+                double* energy_part, int grid, cudaStream_t st, const int32_t* done) {
     if (mk.dim == 2)
-        k_apply_K<2, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part);
+        k_apply_K<2, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
     else
-        k_apply_K<3, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part);
+        k_apply_K<3, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
 }
 template void apply_K_ex<double>(const MeshK&, const double*, const uint8_t*, const double*, double*,
-                                 double*, int, cudaStream_t);
+                                 double*, int, cudaStream_t, const int32_t*);
 template void apply_K_ex<float>(const MeshK&, const float*, const uint8_t*, const float*, float*,
-                                double*, int, cudaStream_t);
+                                double*, int, cudaStream_t, const int32_t*);
 
 template <typename R>
 void apply_K(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y, cudaStream_t st) {
-    apply_K_ex<R>(mk, mom, bcmask, x, y, nullptr, apply_grid(mk.nel), st);
+    apply_K_ex<R>(mk, mom, bcmask, x, y, nullptr, apply_grid(mk.nel), st, nullptr);
     GG_CUDA(cudaGetLastError());
 }
 template void apply_K<double>(const MeshK&, const double*, const uint8_t*, const double*, double*,

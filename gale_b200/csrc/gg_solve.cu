@@ -158,37 +158,16 @@ __global__ void k_cg_direction(int64_t n, const V* __restrict__ z, V* __restrict
 }
 
 template <int DIM, typename V>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(V) == 4 ? 2 : 1)
 k_cg_apply(MeshK mk, const V* __restrict__ mom, const uint8_t* __restrict__ bcmask,
            const V* __restrict__ p, V* __restrict__ Ap, KrylovScalars* s, double* part,
            unsigned int* counter) {
     if (s->done) return;
-    constexpr int NS = 1 << DIM;
-    const int64_t nel = mk.nel, nnode = mk.nnode;
+    const int64_t nel = mk.nel;
     double en = 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        int ijk[3];
-        elem_ijk(mk, e, ijk);
-        int64_t nodes[NS];
-        V u[NS][DIM], yl[NS][DIM];
-#pragma unroll
-        for (int a = 0; a < NS; a++) {
-            nodes[a] = elem_node<DIM>(mk, ijk, a);
-#pragma unroll
-            for (int c = 0; c < DIM; c++) u[a][c] = p[(int64_t)c * nnode + nodes[a]];
-        }
-        element_apply_dev<DIM, V>(mk, mom, nel, e, u, yl);
-#pragma unroll
-        for (int a = 0; a < NS; a++) {
-            const uint8_t bm = bcmask[nodes[a]];
-#pragma unroll
-            for (int c = 0; c < DIM; c++) {
-                en += (double)u[a][c] * (double)yl[a][c];
-                if (!((bm >> c) & 1)) atomicAdd(&Ap[(int64_t)c * nnode + nodes[a]], yl[a][c]);
-            }
-        }
-    }
+         e += (int64_t)gridDim.x * blockDim.x)
+        en += element_apply_scatter<DIM, V>(mk, mom, bcmask, p, Ap, e);
     double acc[1] = {en};
     grid_reduce<1>(acc, part, counter, [=](double* t) {
         s->pAp = t[0];
@@ -198,6 +177,107 @@ k_cg_apply(MeshK mk, const V* __restrict__ mom, const uint8_t* __restrict__ bcma
             s->done = 1;
         }
     });
+}
+
+// ---- flexible CG (truncated FCG) with a multigrid preconditioner ----------------------
+// x = 0, r = b (BC rows zero), p = Ap = 0, rnorm0 = ‖b‖₂; stop when ‖r‖₂ ≤ rtol‖b‖₂
+template <typename V>
+__global__ void k_fcg_init(int64_t n, int64_t nnode, const uint8_t* __restrict__ bcmask, const V* __restrict__ b,
+                           V* __restrict__ x, V* __restrict__ r, V* __restrict__ p, V* __restrict__ Ap, double rtol,
+                           int maxit, KrylovScalars* s, double* part, unsigned int* counter) {
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i / nnode);
+        const bool fixed = (bcmask[i - (int64_t)c * nnode] >> c) & 1;
+        const V rv = fixed ? V(0) : b[i];
+        x[i] = V(0);
+        r[i] = rv;
+        p[i] = V(0);
+        Ap[i] = V(0);
+        acc[0] += (double)rv * (double)rv;
+    }
+    grid_reduce<1>(acc, part, counter, [=](double* t) {
+        s->rnorm0 = sqrt(t[0]);
+        s->rnorm = s->rnorm0;
+        const double tt = rtol * s->rnorm0;
+        s->ttol = tt < 1e-30 ? 1e-30 : tt;
+        s->iterations = 0;
+        s->failed = 0;
+        s->maxit = maxit;
+        s->rz = 0.0;
+        s->done = (s->rnorm0 <= s->ttol) ? 1 : 0;
+    });
+}
+
+// first direction p = z, rz = r·z
+template <typename V>
+__global__ void k_fcg_first(int64_t n, const V* __restrict__ r, const V* __restrict__ z, V* __restrict__ p,
+                            KrylovScalars* s, double* part, unsigned int* counter) {
+    if (s->done) return;
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const V zv = z[i];
+        p[i] = zv;
+        acc[0] += (double)r[i] * (double)zv;
+    }
+    grid_reduce<1>(acc, part, counter, [=](double* t) { s->rz = t[0]; });
+}
+
+// x += αp, r −= αAp, ‖r‖ → convergence (Ap kept for the flexible β)
+template <typename V>
+__global__ void k_fcg_update(int64_t n, V* __restrict__ x, V* __restrict__ r, const V* __restrict__ p,
+                             const V* __restrict__ Ap, KrylovScalars* s, double* part, unsigned int* counter) {
+    if (s->done) return;
+    const V alpha = (V)s->alpha;
+    double acc[1] = {0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        const V rv = r[i] - alpha * Ap[i];  // BC rows of Ap are zero, so r stays zero there
+        r[i] = rv;
+        acc[0] += (double)rv * (double)rv;
+    }
+    grid_reduce<1>(acc, part, counter, [=](double* t) {
+        const double rn = sqrt(t[0]);
+        s->rnorm = rn;
+        s->iterations += 1;
+        if (!(rn == rn) || isinf(rn)) {
+            s->failed = 2;
+            s->done = 1;
+        } else if (rn <= s->ttol) {
+            s->done = 1;
+        } else if (s->iterations >= s->maxit) {
+            s->failed = 1;
+            s->done = 1;
+        }
+    });
+}
+
+// rz = r·z, β = −(z·Ap)/(pᵀAp) (truncated flexible CG, Notay 2000)
+template <typename V>
+__global__ void k_fcg_dots(int64_t n, const V* __restrict__ r, const V* __restrict__ z, const V* __restrict__ Ap,
+                           KrylovScalars* s, double* part, unsigned int* counter) {
+    if (s->done) return;
+    double acc[2] = {0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double zv = (double)z[i];
+        acc[0] += (double)r[i] * zv;
+        acc[1] += zv * (double)Ap[i];
+    }
+    grid_reduce<2>(acc, part, counter, [=](double* t) {
+        s->rz = t[0];
+        s->beta = -t[1] / s->pAp;
+    });
+}
+
+template <typename V>
+__global__ void k_fcg_dir(int64_t n, const V* __restrict__ z, V* __restrict__ p, V* __restrict__ Ap,
+                          const KrylovScalars* s) {
+    if (s->done) return;
+    const V beta = (V)s->beta;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        p[i] = z[i] + beta * p[i];
+        Ap[i] = V(0);
+    }
 }
 
 // ---- generic FP64 vector helpers ----------------------------------------------------
@@ -364,6 +444,91 @@ static int run_cg(Handle& H, const char* key, const MeshK& mk, const V* mom, con
     return GG_OK;
 }
 
+// Multigrid-preconditioned flexible CG in FP32 on the fine level: x = K32⁻¹ b to
+// ‖r‖ ≤ rtol‖b‖.  The V-cycle (and the learned correction when enabled) is part of the
+// captured iteration; `precond` enqueues z = M⁻¹ r.
+template <class Precond>
+static int run_fcg(Handle& H, const char* key, const float* b, float* x, double rtol, int maxit, int* iters,
+                   Precond precond) {
+    constexpr int kChunkMG = 4;
+    Scratch sc = scratch(H);
+    KrylovScalars* ks = H.scal.as<KrylovScalars>();
+    const MeshK& mk = H.mk;
+    const int64_t n = H.ndof;
+    const uint8_t* bcmask = H.bcmask.as<uint8_t>();
+    float* r = H.cgr32.as<float>();
+    float* z = H.z32.as<float>();
+    float* p = H.p32.as<float>();
+    float* Ap = H.Ap32.as<float>();
+    const float* mom = H.mom32.as<float>();
+    const int32_t* done = &ks->done;
+    k_fcg_init<float><<<kRedBlocks, 256, 0, H.stream>>>(n, mk.nnode, bcmask, b, x, r, p, Ap, rtol, maxit, ks, sc.part,
+                                                        sc.counter + 5);
+    GG_CUDA(cudaGetLastError());
+    H.kernel_launches++;
+    char kbuf[200];
+    snprintf(kbuf, sizeof kbuf, "%s:%p:%p:%p:%lld", key, (const void*)b, (void*)x, (void*)ks, (long long)H.build_gen);
+    const std::string kpro = std::string(kbuf) + ":pro", kit = std::string(kbuf) + ":it";
+    auto capture = [&](const std::string& k, auto&& body) {
+        auto it = H.graphs.find(k);
+        if (it != H.graphs.end()) return it->second;
+        cudaGraph_t gph;
+        GG_CUDA(cudaStreamBeginCapture(H.stream, cudaStreamCaptureModeThreadLocal));
+        const int64_t l0 = H.kernel_launches;
+        body();
+        H.graph_nodes[k] = H.kernel_launches - l0;
+        H.kernel_launches = l0;
+        GG_CUDA(cudaStreamEndCapture(H.stream, &gph));
+        cudaGraphExec_t ge;
+        GG_CUDA(cudaGraphInstantiate(&ge, gph, 0));
+        GG_CUDA(cudaGraphDestroy(gph));
+        H.graphs.emplace(k, ge);
+        return ge;
+    };
+    cudaGraphExec_t gpro = capture(kpro, [&]() {
+        precond(r, z, done);
+        k_fcg_first<float><<<kRedBlocks, 256, 0, H.stream>>>(n, r, z, p, ks, sc.part, sc.counter + 6);
+        H.kernel_launches++;
+    });
+    cudaGraphExec_t git = capture(kit, [&]() {
+        const int ga = apply_grid(mk.nel);
+        for (int k = 0; k < kChunkMG; k++) {
+            if (mk.dim == 2)
+                k_cg_apply<2, float><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter + 7);
+            else
+                k_cg_apply<3, float><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter + 7);
+            k_fcg_update<float><<<kRedBlocks, 256, 0, H.stream>>>(n, x, r, p, Ap, ks, sc.part, sc.counter + 5);
+            precond(r, z, done);
+            k_fcg_dots<float><<<kRedBlocks, 256, 0, H.stream>>>(n, r, z, Ap, ks, sc.part, sc.counter + 6);
+            k_fcg_dir<float><<<grid_for(n, 256), 256, 0, H.stream>>>(n, z, p, Ap, ks);
+            H.kernel_launches += 4;
+        }
+    });
+    GG_CUDA(cudaGraphLaunch(gpro, H.stream));
+    H.kernel_launches += H.graph_nodes[kpro];
+    const int64_t max_launches = (int64_t)maxit / kChunkMG + 4;
+    for (int64_t launches = 0;; launches++) {
+        GG_CUDA(cudaMemcpyAsync(H.h_scal, ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, H.stream));
+        GG_CUDA(cudaStreamSynchronize(H.stream));
+        if (H.h_scal->done) break;
+        if (launches > max_launches) return GG_ERR_NOT_CONVERGED;
+        GG_CUDA(cudaGraphLaunch(git, H.stream));
+        GG_CUDA(cudaGetLastError());
+        H.kernel_launches += H.graph_nodes[kit];
+    }
+    *iters = H.h_scal->iterations;
+    if (H.h_scal->failed == 1) return GG_ERR_NOT_CONVERGED;
+    if (H.h_scal->failed) return GG_ERR_NONFINITE;
+    return GG_OK;
+}
+
+int fcg_mg_solve(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters) {
+    int rc = mg_setup(H);
+    if (rc != GG_OK) return rc;
+    return run_fcg(H, "fcg_mg_any", b, x, rtol, maxit, iters,
+                   [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+}
+
 void release_graphs(Handle& H) {
     for (auto& kv : H.graphs) cudaGraphExecDestroy(kv.second);
     H.graphs.clear();
@@ -410,13 +575,43 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
     if (ttol < 1e-50) ttol = 1e-50;
     int total = 0;
     if (rnorm0 <= ttol) { *iters = 0; return GG_OK; }
-    const double inner_rtol = 1e-3;
+    const bool use_mg = prm.inner == GG_INNER_MG_CG || prm.inner == GG_INNER_LEARNED_CG;
+    if (use_mg) {
+        int rc = mg_setup(H);
+        if (rc != GG_OK) return rc;
+    }
+    bool use_nn = prm.inner == GG_INNER_LEARNED_CG && learned_ready(H) && H.nn_enabled;
+    if (use_nn) learned_prepare(H);
+    const double inner_rtol = use_mg ? 1e-4 : 1e-3;
     for (int sweep = 0; sweep < 50; sweep++) {
         k_to_f32<<<grid_for(nd, 256), 256, 0, H.stream>>>(nd, r64, H.r32.as<float>());
         int it = 0;
-        int rc = run_cg<float>(H, "cg32", H.mk, H.mom32.as<float>(), H.kdiag32.as<float>(), H.r32.as<float>(),
+        int rc;
+        if (use_nn) {
+            // learned coarse correction added to the V-cycle; a stagnating solve (no
+            // convergence within kLearnedCap iterations) falls back to plain multigrid
+            constexpr int kLearnedCap = 40;
+            rc = run_fcg(H, "fcg_nn", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, std::min(maxit, kLearnedCap), &it,
+                         [&](const float* rr, float* zz, const int32_t* dn) {
+                             vcycle(H, 0, rr, zz, dn);
+                             learned_correction(H, rr, zz, dn);
+                         });
+            if (rc != GG_OK) {
+                H.fallbacks++;
+                total += it;
+                if (H.fallbacks >= 2) H.nn_enabled = false;  // stop trying for this handle's build
+                use_nn = H.nn_enabled;
+                rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, maxit, &it,
+                             [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+            }
+        } else if (use_mg) {
+            rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, maxit, &it,
+                         [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+        } else {
+            rc = run_cg<float>(H, "cg32", H.mk, H.mom32.as<float>(), H.kdiag32.as<float>(), H.r32.as<float>(),
                                H.e32.as<float>(), H.cgr32.as<float>(), H.z32.as<float>(), H.p32.as<float>(),
                                H.Ap32.as<float>(), inner_rtol, maxit, &it);
+        }
         total += it;
         if (rc == GG_ERR_NONFINITE) return rc;
         // x += e ; r = b − K64 x
@@ -453,6 +648,8 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     const int maxit = prm.inner_max_iterations > 0 ? prm.inner_max_iterations : 10000;
     GG_CUDA(cudaEventRecord(H.ev0, st));
     const int64_t launches0 = H.kernel_launches;
+    H.fallbacks = 0;
+    H.nn_enabled = true;
     int64_t nfree = H.nfree;
     const double scaleq = sqrt((double)ne);
     int rc = GG_OK, it = 0;
@@ -511,7 +708,10 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
         if (!((chosen > prm.tolerance) || (it < prm.min_iterations))) break;
     }
     S.outer_iterations = it;
-    S.kernel_launches = H.kernel_launches - launches0;
+    S.fallbacks = H.fallbacks;
+    // the first solve after a build also accounts for the build's kernels
+    S.kernel_launches = H.kernel_launches - (H.stats_gen != H.build_gen ? H.launches_at_build : launches0);
+    H.stats_gen = H.build_gen;
     S.rel_residual = relres;
     S.abs_residual = absres;
     GG_CUDA(cudaEventRecord(H.ev1, st));

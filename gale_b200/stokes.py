@@ -298,6 +298,38 @@ class StokesProblem:
         self._check(self.lib.gg_courant_dt(self.h, ptr(f64(u)), C.byref(dt)))
         return dt.value
 
+    # learned coarse correction
+    def train_learned(self, level=2, n_rhs=4, iters_per_rhs=6, epochs=60, lr=2e-3, seed=1):
+        p = abi.LearnParams(level, n_rhs, iters_per_rhs, epochs, lr, seed)
+        st = abi.LearnStats()
+        self._check(self.lib.gg_learned_train(self.h, C.byref(p), C.byref(st)))
+        return st.as_dict()
+
+    def learned_weights(self):
+        n = C.c_int32(0)
+        self._check(self.lib.gg_learned_weights(self.h, None, C.byref(n)))
+        w = np.zeros(n.value, dtype=np.float32)
+        self._check(self.lib.gg_learned_weights(self.h, ptr(w, C.c_float), None))
+        return w
+
+    def set_learned_weights(self, w, level=2):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(self.lib.gg_learned_set_weights(self.h, level, ptr(w, C.c_float), w.size))
+
+    def learned_eval(self, inputs, targets, weights, level=2):
+        """Forward + backward of a batch (inputs [B][1+dim][N], targets [B][dim][N])."""
+        x = np.ascontiguousarray(inputs, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        y = np.zeros_like(t)
+        g = np.zeros_like(w)
+        loss = C.c_double(0)
+        nodes = C.c_int32(0)
+        self._check(self.lib.gg_learned_eval(self.h, level, x.shape[0], ptr(x, C.c_float), ptr(t, C.c_float),
+                                             ptr(w, C.c_float), ptr(y, C.c_float), ptr(g, C.c_float),
+                                             C.byref(loss), C.byref(nodes)))
+        return y, g, loss.value
+
     # diagnostics / operator access
     def point_viscosity(self):
         eta = np.zeros(self.np)

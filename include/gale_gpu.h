@@ -177,6 +177,25 @@ typedef struct gg_picard_stats {
     double  solve_ms;
 } gg_picard_stats;
 
+/* Learned coarse correction (no counterpart in the reference): a 2-layer, 32-channel
+ * convolutional network over the nodal grid of one multigrid level, trained on
+ * (viscosity, residual, error) pairs the solver generates on the current operator.     */
+typedef struct gg_learn_params {
+    int32_t level;          /* multigrid level of the network (≤0: level 2 or the coarsest) */
+    int32_t n_rhs;          /* right-hand sides used to generate pairs (force + G s_j)     */
+    int32_t iters_per_rhs;  /* stationary MG iterates recorded per right-hand side         */
+    int32_t epochs;         /* Adam epochs                                                  */
+    float   lr;             /* Adam learning rate                                           */
+    int32_t seed;
+} gg_learn_params;
+
+typedef struct gg_learn_stats {
+    int32_t samples;
+    float   loss_first;     /* mean normalised loss of the first / last epoch              */
+    float   loss_last;
+    double  train_ms;
+} gg_learn_stats;
+
 typedef struct gg_handle gg_handle;
 
 /* ---- lifetime -------------------------------------------------------------------
@@ -271,6 +290,19 @@ GG_API int  gg_apply_GT(gg_handle* h, const double* u, double* q);
 GG_API int  gg_get_rhs(gg_handle* h, double* f, double* hvec);
 /* Diagonal of the assembled K [nodes*dim] and of Ĝ [elements].                        */
 GG_API int  gg_get_diagonals(gg_handle* h, double* k_diag, double* schur_diag);
+/* ---- learned coarse correction (no counterpart in the reference) ----------------------
+ * gg_learned_train needs an operator built with GG_PRECISION_MIXED.  Weights are FP32
+ * on the host side of the ABI; the device runs them in BF16.  n: parameter count.      */
+GG_API int  gg_learned_train(gg_handle* h, const gg_learn_params* params, gg_learn_stats* stats);
+GG_API int  gg_learned_weights(gg_handle* h, float* weights, int32_t* n);
+GG_API int  gg_learned_set_weights(gg_handle* h, int32_t level, const float* weights, int32_t n);
+/* Forward and backward of a batch on the network's grid (gradient check): inputs
+ * [batch][1+dim][nodes], targets [batch][dim][nodes]; writes outputs, the gradient of
+ * the normalised loss w.r.t. all parameters, the loss and the grid's node count.     */
+GG_API int  gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const float* inputs,
+                            const float* targets, const float* weights, float* outputs,
+                            float* gradient, double* loss, int32_t* grid_nodes);
+
 /* Measurement only (no reference counterpart): average device time of one matrix-free
  * K apply over `reps` back-to-back launches on the handle's stream, CUDA events.       */
 GG_API int  gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_launch);

@@ -1,0 +1,103 @@
+"""Learned coarse correction: gradients against the CPU reference, training, and what the
+trained network gains in the inner solve (needs a B200)."""
+import numpy as np
+import pytest
+
+from gale_b200 import workloads
+from gale_b200.stokes import StokesProblem, UzawaSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(a):
+    """Round float32 to bfloat16 (nearest, ties to even) and back."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def split(w, dim, hidden=32):
+    cin, cout, taps = 1 + dim, dim, (27 if dim == 3 else 9)
+    n1w, n1b, n2w = hidden * taps * cin, hidden, cout * taps * hidden
+    W1 = w[:n1w].reshape(hidden, taps, cin)
+    b1 = w[n1w:n1w + n1b]
+    W2 = w[n1w + n1b:n1w + n1b + n2w].reshape(cout, taps, hidden)
+    b2 = w[n1w + n1b + n2w:]
+    return W1, b1, W2, b2
+
+
+def level_grid(mesh, level):
+    return tuple(int(mesh.elements[d] // (1 << level)) + 1 if d < mesh.dim else 1 for d in range(3))
+
+
+@pytest.mark.parametrize("make,level", [(lambda: workloads.creep_3d(n=16), 2),
+                                        (lambda: workloads.sinker_2d(n=32), 2)], ids=["3d", "2d"])
+def test_gradients_match_cpu_reference(make, level):
+    from oracle import learned_ref
+    w = make()
+    G = w.apply(StokesProblem(w.mesh))
+    G.locate()
+    G.build_operator("mixed")
+    dim = w.dim
+    grid = level_grid(w.mesh, level)
+    N = int(np.prod(grid))
+    rng = np.random.default_rng(5)
+    P = G.learned_weights().size
+    weights = (0.2 * rng.standard_normal(P)).astype(np.float32)
+    B = 3
+    x = rng.standard_normal((B, 1 + dim, N)).astype(np.float32)
+    t = rng.standard_normal((B, dim, N)).astype(np.float32)
+    y, g, loss = G.learned_eval(x, t, weights, level=level)
+    # the free-dof mask of the level: nodes on walls with a fixed normal component
+    mask = np.ones((dim, N))
+    idx = np.indices(grid[::-1]).reshape(3, -1)[::-1]  # x, y, z per node
+    for c in range(dim):
+        mask[c, idx[c] == 0] = 0
+        mask[c, idx[c] == grid[c] - 1] = 0
+    W1, b1, W2, b2 = split(weights.astype(np.float64), dim)
+    W1r, W2r = bf16(W1.astype(np.float32)).astype(np.float64), bf16(W2.astype(np.float32)).astype(np.float64)
+    yr, lr, (dW1, db1, dW2, db2) = learned_ref.forward_backward(
+        x.astype(np.float64), t.astype(np.float64) * mask[None], mask, W1r, b1, W2r, b2, grid, dim)
+    # targets at BC dofs are ignored by the masked loss on both sides
+    assert np.linalg.norm(y - yr) <= 1e-4 * np.linalg.norm(yr)
+    assert abs(loss - lr) <= 1e-4 * abs(lr)
+    gr = np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2])
+    assert np.linalg.norm(g - gr) <= 1e-3 * np.linalg.norm(gr)
+
+
+def test_training_and_gain():
+    w = workloads.creep_3d(n=32)
+    G = w.apply(StokesProblem(w.mesh))
+    G.locate()
+    G.build_operator("mixed")
+    st = G.train_learned(level=2, n_rhs=4, iters_per_rhs=6, epochs=40)
+    assert st["samples"] == 24
+    assert st["loss_last"] < st["loss_first"]
+    # plain multigrid vs multigrid + learned correction, same Uzawa tolerance
+    u0, p0, s0 = G.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="mg"))
+    u1, p1, s1 = G.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="learned"))
+    assert s1["rel_residual"] <= 1e-6 and s0["rel_residual"] <= 1e-6
+    assert np.linalg.norm(u1 - u0) / np.linalg.norm(u0) < 1e-3
+    gain = s0["inner_iterations"] / max(1, s1["inner_iterations"])
+    print(f"learned gain: inner iterations {s0['inner_iterations']} -> {s1['inner_iterations']} "
+          f"(x{gain:.2f}), solve {s0['solve_ms']:.1f} -> {s1['solve_ms']:.1f} ms, "
+          f"fallbacks {s1['fallbacks']}, loss {st['loss_first']:.3f} -> {st['loss_last']:.3f}")
+    # the learned path must not cost more inner iterations than plain multigrid
+    assert s1["inner_iterations"] <= 1.05 * s0["inner_iterations"]
+
+
+def test_weights_transfer_between_instances():
+    a = workloads.creep_3d(n=16, seed=11)
+    b = workloads.creep_3d(n=16, seed=12)
+    GA = a.apply(StokesProblem(a.mesh))
+    GA.locate()
+    GA.build_operator("mixed")
+    GA.train_learned(level=2, epochs=10)
+    wts = GA.learned_weights()
+    GB = b.apply(StokesProblem(b.mesh))
+    GB.locate()
+    GB.build_operator("mixed")
+    GB.set_learned_weights(wts, level=2)
+    assert np.array_equal(GB.learned_weights(), wts)
+    _, _, s = GB.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="learned"))
+    assert s["rel_residual"] <= 1e-6
