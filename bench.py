@@ -172,14 +172,15 @@ def gale_arm(args):
     if not args.no_accuracy:
         # the discrete solution: plain FP64 path at tight tolerances (= the oracle to 1e-10)
         G.build_operator("fp64")
-        ut, pt, st_t = G.solve(UzawaSolver(tolerance=1e-9, precision="fp64", inner="jacobi",
-                                           innerRtolFactor=0.01))
+        ut, pt, st_t = G.solve(UzawaSolver(tolerance=1e-8, precision="fp64", inner="jacobi",
+                                           innerRtolFactor=0.01, innerMaxIterations=200000))
         # the headline path tightened until its error matches 1e-6
         acc_prm = UzawaSolver(tolerance=args.accurate_rtol, precision="mixed", inner=args.inner,
                               innerRtolFactor=0.01)
         t_acc, st_acc, (ua, pa) = timed(acc_prm, "mixed", 1, 1)
         accuracy = {
-            "reference": "plain FP64 path at Uzawa rtol 1e-9, inner rtol 1e-11",
+            "reference": "plain FP64 path at Uzawa rtol 1e-8, inner rtol 1e-10",
+            "reference_iterations": {k: st_t[k] for k in ("outer_iterations", "inner_iterations")},
             "headline_rtol1e-6": {"u": rel(uh, ut), "p": rel(ph, pt, True)},
             "plain_fp64_rtol1e-6": {"u": rel(u64, ut), "p": rel(p64, pt, True)},
             "headline_tight": {"uzawa_rtol": args.accurate_rtol, "inner_rtol": 0.01 * args.accurate_rtol,
@@ -331,14 +332,34 @@ def main():
     ap.add_argument("--cpu-sample-its", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--profile-solve", type=float, default=None, metavar="RTOL",
+                    help="build + one solve at this Uzawa rtol, no timing (ncu captures)")
+    ap.add_argument("--fp64", action="store_true", help="with --profile-solve --inner jacobi: plain FP64 path")
     ap.add_argument("--accurate-rtol", type=float, default=1e-8)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+    elif args.profile_solve is not None:
+        profile_solve(args)
     else:
         gale_arm(args)
+
+
+def profile_solve(args):
+    """One operator build + one solve of the workload, no timing (for ncu captures; a loose
+    Uzawa tolerance keeps the launch count small while the per-iteration kernel mix stays
+    the one of the benchmark solve)."""
+    from gale_b200 import workloads
+    from gale_b200.stokes import StokesProblem, UzawaSolver
+    w = workloads.creep_3d(n=args.n)
+    G = w.apply(StokesProblem(w.mesh))
+    G.locate()
+    prec = "fp64" if args.inner == "jacobi" and args.fp64 else "mixed"
+    G.build_operator(prec)
+    _, _, st = G.solve(UzawaSolver(tolerance=args.profile_solve, precision=prec, inner=args.inner))
+    print(json.dumps(st))
 
 
 if __name__ == "__main__":

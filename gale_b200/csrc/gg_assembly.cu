@@ -25,8 +25,6 @@
 
 namespace gg {
 
-__constant__ MaterialTable c_materials;
-
 namespace {
 
 constexpr int kElemPerCta = 128;
@@ -216,7 +214,8 @@ k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
                 double gravity, double g0, double g1, double g2, double rayleigh, int want_force,
                 R* __restrict__ mom, R* __restrict__ kdiag, double* __restrict__ sdiag,
                 double* __restrict__ f, double* __restrict__ eta_s, double* __restrict__ incr_s,
-                uint8_t* __restrict__ yld_s, int32_t* __restrict__ flag) {
+                uint8_t* __restrict__ yld_s, int32_t* __restrict__ flag,
+                const gg_material* __restrict__ materials) {
     constexpr int NM = n_moments<DIM>();
     constexpr int NEN = 1 << DIM;
     __shared__ R s_c[kChunk];
@@ -257,7 +256,7 @@ k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
 #pragma unroll
             for (int d = 0; d < DIM; d++) xi[d] = (R)xi_s[(int64_t)d * np_s + i];
             const int mi = mat_s[i];
-            const gg_material& m = c_materials.m[mi];
+            const gg_material& m = materials[mi];
             PointOut po = run_rheologies<DIM, R>(mk, m, ijk, pe, xi, T, pu, pp, ps_s[i], prev);
             const int32_t cnt = offsets[pe + 1] - offsets[pe];
             const double w = wscale / (double)cnt;  // _ConstantWeights_Calculate
@@ -379,11 +378,13 @@ k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
 
 }  // namespace
 
+// The material table lives in a per-handle device buffer, so concurrent handles (threads,
+// streams) never share it.
 void upload_materials(Handle& H) {
-    MaterialTable t{};
-    t.n = H.n_materials;
-    for (int i = 0; i < H.n_materials; i++) t.m[i] = H.materials[i];
-    GG_CUDA(cudaMemcpyToSymbolAsync(c_materials, &t, sizeof(t), 0, cudaMemcpyHostToDevice, H.stream));
+    H.d_materials.ensure(sizeof(gg_material) * GG_MAX_MATERIALS);
+    H.h_materials.assign(H.materials.begin(), H.materials.end());
+    GG_CUDA(cudaMemcpyAsync(H.d_materials.p, H.h_materials.data(), sizeof(gg_material) * H.h_materials.size(),
+                            cudaMemcpyHostToDevice, H.stream));
 }
 
 template <int DIM, typename R>
@@ -397,7 +398,7 @@ static void launch_build(Handle& H, int prev, const double* pu, const double* pp
         H.mk, nel, H.offsets.as<int32_t>(), H.xi_s.as<double>(), H.np_in, H.mat_s.as<int32_t>(),
         H.ps_s.as<double>(), T, pu, pp, prev, H.force.gravity, g[0], g[1], g[2], H.force.rayleigh,
         f ? 1 : 0, mom, kdiag, sdiag, f, outputs ? H.eta_s.as<double>() : nullptr,
-        H.incr_s.as<double>(), H.yld_s.as<uint8_t>(), H.flag.as<int32_t>());
+        H.incr_s.as<double>(), H.yld_s.as<uint8_t>(), H.flag.as<int32_t>(), H.d_materials.as<gg_material>());
     GG_CUDA(cudaGetLastError());
 }
 

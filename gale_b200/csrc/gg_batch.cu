@@ -1,0 +1,63 @@
+// gg_batch.cu -- many independent Stokes problems at once (the uneven batched sweep).
+//
+// Gale solves one problem per run (one SLE per MPI job).  Here a batch of independent
+// problems of different mesh sizes is driven from a shared work queue: `workers` host
+// threads pull the next problem index from an atomic counter and run locate → build →
+// Uzawa on that problem's handle.  Every handle owns its CUDA stream and CUDA graphs, so
+// the small, latency-bound kernels of different problems overlap on the GPU's 148 SMs
+// instead of running one problem after another.
+#include <atomic>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+
+namespace gg {
+int build_all(Handle& H, int precision, int prev, const double* d_u, const double* d_p);
+void store_solution(Handle& H);
+}  // namespace gg
+
+namespace {
+
+int solve_one(gg_handle* h, const gg_uzawa_params* prm, double* u, double* p, gg_uzawa_stats* st) {
+    int rc = gg_locate(h, nullptr);
+    if (rc != GG_OK) return rc;
+    rc = gg_build_operator(h, prm->precision, 0, nullptr, nullptr);
+    if (rc != GG_OK) return rc;
+    return gg_uzawa_solve(h, prm, u, p, st);
+}
+
+}  // namespace
+
+extern "C" int gg_solve_batch(int32_t n, gg_handle* const* handles, const gg_uzawa_params* params,
+                              int32_t workers, double* const* u_out, double* const* p_out,
+                              gg_uzawa_stats* stats, int32_t* status) {
+    if (n < 1 || !handles || !params || !u_out || !p_out || !status) return GG_ERR_INVALID;
+    for (int i = 0; i < n; i++)
+        if (!handles[i] || !u_out[i] || !p_out[i]) return GG_ERR_INVALID;
+    if (workers < 1) workers = 1;
+    if (workers > n) workers = n;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GG_ERR_NO_DEVICE;
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        cudaSetDevice(dev);
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            gg_uzawa_stats st;
+            std::memset(&st, 0, sizeof st);
+            status[i] = solve_one(handles[i], params, u_out[i], p_out[i], &st);
+            if (stats) stats[i] = st;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; w++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (int i = 0; i < n; i++)
+        if (status[i] != GG_OK) return status[i];
+    return GG_OK;
+}

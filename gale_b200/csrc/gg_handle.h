@@ -72,6 +72,8 @@ struct Handle {
     gg_body_force force{};
     int n_materials = 0;
     std::vector<gg_material> materials;
+    std::vector<gg_material> h_materials;  // staging copy for the async upload
+    DBuf d_materials;
 
     // points
     int64_t np = 0, np_in = 0;

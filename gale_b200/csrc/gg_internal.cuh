@@ -79,10 +79,5 @@ __host__ __device__ constexpr int mom_slot(int a, int b, int c) {
     return DIM == 2 ? mom_slot2(a, b) : mom_slot3(a, b, c);
 }
 
-// Device copy of the material table (constant memory, defined in gg_assembly.cu).
-struct MaterialTable {
-    int n;
-    gg_material m[GG_MAX_MATERIALS];
-};
 
 }  // namespace gg

@@ -298,12 +298,36 @@ class StokesProblem:
         self._check(self.lib.gg_courant_dt(self.h, ptr(f64(u)), C.byref(dt)))
         return dt.value
 
+    @staticmethod
+    def solve_batch(problems, params: abi.UzawaParams, workers: int = 16):
+        """locate → build → Uzawa for every problem (inputs set), `workers` host threads
+        feeding one GPU.  Returns [(u, p, stats)] and raises on the first failure."""
+        n = len(problems)
+        lib = problems[0].lib
+        hs = (C.c_void_p * n)(*[pr.h for pr in problems])
+        us = [np.zeros(pr.nnode * pr.dim) for pr in problems]
+        ps = [np.zeros(pr.nel) for pr in problems]
+        up = (C.POINTER(C.c_double) * n)(*[ptr(u) for u in us])
+        pp = (C.POINTER(C.c_double) * n)(*[ptr(p) for p in ps])
+        st = (abi.UzawaStats * n)()
+        status = np.zeros(n, dtype=np.int32)
+        rc = lib.gg_solve_batch(n, hs, C.byref(params), workers, up, pp, st, ptr(status, C.c_int32))
+        if rc != 0:
+            bad = int(np.flatnonzero(status)[0])
+            raise GaleError(rc, f"problem {bad}: " + lib.gg_last_error(problems[bad].h).decode())
+        return [(us[i], ps[i], st[i].as_dict()) for i in range(n)]
+
     # learned coarse correction
     def train_learned(self, level=2, n_rhs=4, iters_per_rhs=6, epochs=60, lr=2e-3, seed=1):
         p = abi.LearnParams(level, n_rhs, iters_per_rhs, epochs, lr, seed)
         st = abi.LearnStats()
         self._check(self.lib.gg_learned_train(self.h, C.byref(p), C.byref(st)))
         return st.as_dict()
+
+    def learned_param_count(self):
+        n = C.c_int32(0)
+        self._check(self.lib.gg_learned_weights(self.h, None, C.byref(n)))
+        return n.value
 
     def learned_weights(self):
         n = C.c_int32(0)

@@ -263,6 +263,16 @@ GG_API int  gg_uzawa_solve(gg_handle* h, const gg_uzawa_params* params, double* 
 GG_API int  gg_picard(gg_handle* h, const gg_picard_params* picard, const gg_uzawa_params* uzawa,
                double* u, double* p, gg_picard_stats* stats);
 
+/* Batch of independent problems (uneven sizes): for every handle (inputs already set)
+ * locate → build → Uzawa, pulled from a shared work queue by `workers` host threads; each
+ * handle runs on its own stream so the problems overlap on the GPU.  Gale runs one SLE
+ * per job; the batch form has no single reference counterpart (it replaces running
+ * _Stokes_SLE_UzawaSolver_Solve once per job).  status[i] gets each problem's status;
+ * the return value is the first non-zero status.                                        */
+GG_API int  gg_solve_batch(int32_t n, gg_handle* const* handles, const gg_uzawa_params* params,
+                           int32_t workers, double* const* u_out, double* const* p_out,
+                           gg_uzawa_stats* stats, int32_t* status);
+
 /* ---- advection ---------------------------------------------------------------------
  * Replaces TimeIntegrand_SecondOrder / first order (StgDomain/Utils/src/
  * TimeIntegrand.cxx:265-335, :457-483) with _SwarmAdvector_TimeDeriv

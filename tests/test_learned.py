@@ -42,7 +42,7 @@ def test_gradients_match_cpu_reference(make, level):
     grid = level_grid(w.mesh, level)
     N = int(np.prod(grid))
     rng = np.random.default_rng(5)
-    P = G.learned_weights().size
+    P = G.learned_param_count()
     weights = (0.2 * rng.standard_normal(P)).astype(np.float32)
     B = 3
     x = rng.standard_normal((B, 1 + dim, N)).astype(np.float32)
