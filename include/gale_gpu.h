@@ -235,6 +235,23 @@ GG_API int  gg_set_body_force(gg_handle* h, const gg_body_force* force);
  * GG_ERR_OUT_OF_DOMAIN and get cell = element count (ElementCellLayout.cxx:266-275). */
 GG_API int  gg_locate(gg_handle* h, uint32_t* owning_cell);
 
+/* No-allocation point location (no counterpart in the reference).  For callers that
+ * cannot allocate device memory (a host that owns all memory through its own allocator
+ * or a fixed arena, real-time drivers that forbid allocation after start-up): the same
+ * bit-exact search, per-element offsets and stable per-element point order as gg_locate,
+ * computed on device buffers the caller owns, without a handle and without any
+ * allocation.  Inputs/outputs are device pointers: d_coords [n_points*dim], d_cell
+ * [n_points] (element count for points outside), d_offsets [elements+1], d_order
+ * [n_points] (point indices grouped by element, ascending inside each element).  Limits:
+ * at most 1,048,576 elements and 1024 points per element (GG_ERR_INVALID otherwise, with
+ * *message set).  The counting-sort scratch is one fixed device array shared by every
+ * call on a device: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on each device performs a one-time set-up (the array's device
+ * address); make it before any stream capture.  stream: a cudaStream_t (NULL: default).  */
+GG_API int  gg_locate_noalloc(const gg_mesh_desc* mesh, int64_t n_points, const double* d_coords,
+                              uint32_t* d_cell, int32_t* d_offsets, int32_t* d_order,
+                              int64_t* n_outside, void* stream, const char** message);
+
 /* ---- operator build ---------------------------------------------------------------
  * Replaces the assembleStiffnessMatrix entry point (__StiffnessMatrix_NewAssemble,
  * StiffnessMatrix.cxx:2016-2200) for k_matrix, g_matrix and the Uzawa preconditioner,
