@@ -113,12 +113,10 @@ def gale_arm(args):
         if world > 1:
             dist.barrier()
 
+    from gale_b200.replicas import max_over_ranks as _max
+
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return _max(v, device="cuda")
 
     from gale_b200 import abi, workloads
     from gale_b200.stokes import StokesProblem, UzawaSolver
@@ -335,6 +333,10 @@ def main():
     ap.add_argument("--profile-solve", type=float, default=None, metavar="RTOL",
                     help="build + one solve at this Uzawa rtol, no timing (ncu captures)")
     ap.add_argument("--fp64", action="store_true", help="with --profile-solve --inner jacobi: plain FP64 path")
+    ap.add_argument("--config", default="creep", choices=["creep", "batch"])
+    ap.add_argument("--batch", type=int, default=512)
+    ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--serial-sample", type=int, default=24)
     ap.add_argument("--accurate-rtol", type=float, default=1e-8)
     args = ap.parse_args()
     if args.warmup < 3:
@@ -343,8 +345,60 @@ def main():
         reference_arm(args)
     elif args.profile_solve is not None:
         profile_solve(args)
+    elif args.config == "batch":
+        batch_arm(args)
     else:
         gale_arm(args)
+
+
+def batch_arm(args):
+    """Uneven batched sweep: independent 2D sinkers (n ∈ {32,48,64,96,128}², contrast
+    1–1e4, radius 0.05–0.2, 20 points/element), sharded over ranks; on each GPU all its
+    problems run through gg_solve_batch (one work queue, `--workers` concurrent problems,
+    FP32/FP64 + multigrid).  Reported against one problem at a time on the plain FP64 path
+    (measured on the first `--serial-sample` problems)."""
+    import torch
+    import torch.distributed as dist
+    from gale_b200 import workloads
+    from gale_b200.replicas import max_over_ranks, shard, sum_over_ranks
+    from gale_b200.stokes import StokesProblem, UzawaSolver
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    ws = shard(workloads.batch_sinkers(count=args.batch), rank, world)
+    probs = [w.apply(StokesProblem(w.mesh)) for w in ws]
+    fast = UzawaSolver(tolerance=1e-5, precision="mixed", inner="mg")
+    StokesProblem.solve_batch(probs[:min(8, len(probs))], fast, workers=args.workers)  # warm-up
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = StokesProblem.solve_batch(probs, fast, workers=args.workers)
+    torch.cuda.synchronize()
+    t_batch = max_over_ranks(time.perf_counter() - t0, device="cuda")
+    total = sum_over_ranks(len(probs), device="cuda")
+    per = np.array([st["solve_ms"] for _, _, st in res])
+    ns = min(args.serial_sample, len(probs))
+    plain = UzawaSolver(tolerance=1e-5, precision="fp64", inner="jacobi")
+    t0 = time.perf_counter()
+    ser = StokesProblem.solve_batch(probs[:ns], plain, workers=1)
+    t_serial = (time.perf_counter() - t0) / ns
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "batched uneven sweep: solves/s", "value": total / t_batch, "unit": "solves/s",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64", "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": f"{args.batch} 2D sinkers n in {{32,48,64,96,128}}^2, 20 ppc, Uzawa rtol 1e-5",
+                       "workers": args.workers, "parallelism": f"problems sharded x{world}"},
+            "batch_wall_s": t_batch,
+            "per_problem_solve_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+            "one_at_a_time_plain_fp64_s_per_problem": t_serial,
+            "speedup_vs_one_at_a_time": t_serial * total / t_batch,
+            "serial_sample": ns}), flush=True)
 
 
 def profile_solve(args):

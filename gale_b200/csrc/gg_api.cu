@@ -441,7 +441,9 @@ int gg_uzawa_solve(gg_handle* h, const gg_uzawa_params* prm, double* u, double* 
         H.have_solution = true;
     })
     if (stats) *stats = S;
-    if (rc != GG_OK) gg::set_error(H, rc, "Uzawa solve failed (status " + std::to_string(rc) + ")");
+    if (rc != GG_OK)
+        gg::set_error(H, rc, "Uzawa solve failed (status " + std::to_string(rc) + ")" +
+                                 (H.fail_where.empty() ? std::string() : ": " + H.fail_where));
     return rc;
 }
 

@@ -64,6 +64,7 @@ struct Handle {
     int64_t nel = 0, nnode = 0, ndof = 0;
     cudaStream_t stream = nullptr;
     std::string err;
+    std::string fail_where;  // stage at which the last Uzawa solve stopped early
 
     // mesh-level data
     DBuf bcmask, bcval, T;
@@ -106,6 +107,7 @@ struct Handle {
     bool nn_ready = false;
     bool nn_enabled = true;    // cleared after repeated stagnation (fallback to multigrid)
     int fallbacks = 0;         // learned → multigrid fallbacks taken in the current solve
+    int calib_mg = 0, calib_nn = 0;  // FCG iterations of the calibration solves (learned vs MG)
     int nn_level = 2;       // hierarchy level the network acts on
     DBuf mg_xs, mg_xk, mg_xt;  // FP32 fine-level scratch of the training data generator
 

@@ -54,7 +54,7 @@ void apply_GT(const Handle& H, const double* u, double* q, cudaStream_t st);
 // Krylov / Uzawa (gg_solve.cu)
 int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& st);
 int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* x,
-                double rtol, int maxit, int* iters);
+                double rtol, int maxit, int* iters, bool warm = false);
 void release_graphs(Handle& H);
 
 // Multigrid (gg_mg.cu): hierarchy for the current build; z = M⁻¹ b on level l.

@@ -259,6 +259,13 @@ __global__ void k_nn_output(int64_t N, int dim, const uint8_t* __restrict__ bc, 
     }
 }
 
+__global__ void k_resid_after(int64_t n, const float* __restrict__ r, const float* __restrict__ t,
+                              float* __restrict__ out, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = r[i] - t[i];
+}
+
 __global__ void k_zero(int64_t n, float* __restrict__ a, const int32_t* __restrict__ done) {
     if (done && *done) return;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) a[i] = 0.f;
@@ -280,6 +287,7 @@ struct LearnedState {
     DBuf logeta;                          // standardised level-L log10 η [N]
     std::vector<std::unique_ptr<DBuf>> rl, el;  // per-level restricted residual / correction
     DBuf xin, h, pre, y, scale;                 // inference buffers (batch 1)
+    DBuf t0, r0;                                // fine-level A z and r − A z
     int64_t gen = -1;                           // build generation of logeta
 };
 
@@ -308,6 +316,8 @@ static void ensure_net(Handle& H, size_t level) {
     S.pre.ensure(sizeof(float) * kHidden * N);
     S.y.ensure(sizeof(float) * dim * N);
     S.scale.ensure(sizeof(float) * 4);
+    S.t0.ensure(sizeof(float) * H.ndof);
+    S.r0.ensure(sizeof(float) * H.ndof);
     if (S.rl.size() != level + 1) {
         S.rl.clear();
         S.el.clear();
@@ -355,7 +365,13 @@ void learned_correction(Handle& H, const float* r, float* z, const int32_t* done
     LearnedState& S = learned(H);
     const size_t Lv = S.level;
     const int dim = H.dim;
-    const float* src = r;
+    // residual the V-cycle leaves: r' = r − A z
+    MGLevel& L0 = *H.mg[0];
+    k_zero<<<g(H.ndof), 256, 0, H.stream>>>(H.ndof, S.t0.as<float>(), done);
+    apply_K_ex<float>(L0.mk, L0.mom32, L0.bcmask, z, S.t0.as<float>(), nullptr, apply_grid(L0.nel), H.stream, done);
+    k_resid_after<<<g(H.ndof), 256, 0, H.stream>>>(H.ndof, r, S.t0.as<float>(), S.r0.as<float>(), done);
+    H.kernel_launches += 3;
+    const float* src = S.r0.as<float>();
     for (size_t l = 1; l <= Lv; l++) {
         mg_restrict(H, l, src, S.rl[l]->as<float>(), done);
         src = S.rl[l]->as<float>();
@@ -598,8 +614,16 @@ int learned_train(Handle& H, const gg_learn_params& P, gg_learn_stats& st) {
             train_residual(H, b32, xk, rk);
             vcycle(H, 0, rk, zk, nullptr);
             train_target(H, xs, xk, zk, tk);
-            // restrict r to level L → input, inject t → target
-            const float* src = rk;
+            // input: the residual the V-cycle leaves, r' = r − A z (target t = A⁻¹ r');
+            // restricted to level L; target t injected to level L
+            {
+                MGLevel& L0 = *H.mg[0];
+                k_zero<<<g(nd), 256, 0, H.stream>>>(nd, S.t0.as<float>(), nullptr);
+                apply_K_ex<float>(L0.mk, L0.mom32, L0.bcmask, zk, S.t0.as<float>(), nullptr, apply_grid(L0.nel),
+                                  H.stream, nullptr);
+                k_resid_after<<<g(nd), 256, 0, H.stream>>>(nd, rk, S.t0.as<float>(), S.r0.as<float>(), nullptr);
+            }
+            const float* src = S.r0.as<float>();
             for (size_t l = 1; l <= S.level; l++) {
                 mg_restrict(H, l, src, S.rl[l]->as<float>(), nullptr);
                 src = S.rl[l]->as<float>();

@@ -546,7 +546,7 @@ static void ensure_solver_buffers(Handle& H, bool mixed) {
 
 // x = K⁻¹ b (device FP64 vectors), stopping rule of the reference's inner KSP.
 int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* x, double rtol,
-                int maxit, int* iters) {
+                int maxit, int* iters, bool warm) {
     const int64_t nd = H.ndof;
     const uint8_t* bcmask = H.bcmask.as<uint8_t>();
     if (prm.precision == GG_PRECISION_FP64) {
@@ -563,18 +563,34 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
     double* r64 = H.cg_r.as<double>();
     double* bb = H.cg_b.as<double>();
     GG_CUDA(cudaMemcpyAsync(bb, b, sizeof(double) * nd, cudaMemcpyDeviceToDevice, H.stream));
-    GG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * nd, H.stream));
-    // rnorm0 = ‖D⁻¹ b‖ on free rows
+    if (!warm) GG_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * nd, H.stream));
+    // rnorm0 = ‖D⁻¹ b‖ on free rows (the stopping rule is relative to b, as from a zero guess)
     GG_CUDA(cudaMemsetAsync(r64, 0, sizeof(double) * nd, H.stream));
     k_defect<<<kRedBlocks, 256, 0, H.stream>>>(nd, H.nnode, bcmask, bb, H.kdiag64.as<double>(), r64,
                                                 sc.part, sc.counter + 4, sc.out + 1);
+    H.kernel_launches++;
     double rnorm0;
     GG_CUDA(cudaMemcpyAsync(&rnorm0, sc.out + 1, sizeof(double), cudaMemcpyDeviceToHost, H.stream));
     GG_CUDA(cudaStreamSynchronize(H.stream));
     double ttol = rtol * rnorm0;
     if (ttol < 1e-50) ttol = 1e-50;
     int total = 0;
-    if (rnorm0 <= ttol) { *iters = 0; return GG_OK; }
+    if (warm) {
+        // initial guess x0: r = b − K64 x0
+        GG_CUDA(cudaMemsetAsync(r64, 0, sizeof(double) * nd, H.stream));
+        apply_K<double>(H.mk, H.mom64.as<double>(), bcmask, x, r64, H.stream);
+        k_defect<<<kRedBlocks, 256, 0, H.stream>>>(nd, H.nnode, bcmask, bb, H.kdiag64.as<double>(), r64,
+                                                    sc.part, sc.counter + 4, sc.out + 1);
+        H.kernel_launches += 2;
+        double rn;
+        GG_CUDA(cudaMemcpyAsync(&rn, sc.out + 1, sizeof(double), cudaMemcpyDeviceToHost, H.stream));
+        GG_CUDA(cudaStreamSynchronize(H.stream));
+        if (!(rn == rn)) return GG_ERR_NONFINITE;
+        if (rn <= ttol) { *iters = 0; return GG_OK; }
+    } else if (rnorm0 <= ttol) {
+        *iters = 0;
+        return GG_OK;
+    }
     const bool use_mg = prm.inner == GG_INNER_MG_CG || prm.inner == GG_INNER_LEARNED_CG;
     if (use_mg) {
         int rc = mg_setup(H);
@@ -583,6 +599,11 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
     bool use_nn = prm.inner == GG_INNER_LEARNED_CG && learned_ready(H) && H.nn_enabled;
     if (use_nn) learned_prepare(H);
     const double inner_rtol = use_mg ? 1e-4 : 1e-3;
+    // One FP32 sweep stops at inner_rtol or at sweep_cap iterations, whichever comes first;
+    // a capped sweep still reduces the defect and the FP64 refinement below carries on from
+    // it.  The cap keeps an FP32 solve that has hit its rounding floor (large viscosity
+    // contrasts) from spending the whole iteration budget in one sweep.
+    const int sweep_cap = use_mg ? std::min(maxit, 150) : maxit;
     for (int sweep = 0; sweep < 50; sweep++) {
         k_to_f32<<<grid_for(nd, 256), 256, 0, H.stream>>>(nd, r64, H.r32.as<float>());
         int it = 0;
@@ -601,11 +622,11 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
                 total += it;
                 if (H.fallbacks >= 2) H.nn_enabled = false;  // stop trying for this handle's build
                 use_nn = H.nn_enabled;
-                rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, maxit, &it,
+                rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it,
                              [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
             }
         } else if (use_mg) {
-            rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, maxit, &it,
+            rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it,
                          [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
         } else {
             rc = run_cg<float>(H, "cg32", H.mk, H.mom32.as<float>(), H.kdiag32.as<float>(), H.r32.as<float>(),
@@ -653,17 +674,51 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     int64_t nfree = H.nfree;
     const double scaleq = sqrt((double)ne);
     int rc = GG_OK, it = 0;
-    auto inner = [&](const double* b, double* x, double rtol) {
+    auto inner = [&](const double* b, double* x, double rtol, bool warm = false) {
         int its = 0;
-        int r2 = inner_solve(H, prm, b, x, rtol, maxit, &its);
+        int r2 = inner_solve(H, prm, b, x, rtol, maxit, &its, warm);
         S.inner_iterations += its;
         S.inner_solves++;
         return r2;
     };
+    H.fail_where.clear();
+    // an early exit still reports how far the solve got
+    auto fail = [&](const char* where, int code) {
+        S.outer_iterations = it;
+        S.fallbacks = H.fallbacks;
+        H.fail_where = std::string(where) + " at outer iteration " + std::to_string(it) + " (" +
+                       std::to_string(S.inner_iterations) + " inner iterations so far)";
+        return code;
+    };
     const double fnorm = sqrt(dot(H, nd, f, f));
     if (fnorm / sqrt((double)nfree) <= 1e-99) return GG_ERR_ZERO_FORCE;
+    if (prm.inner == GG_INNER_LEARNED_CG && learned_ready(H)) {
+        // the plain multigrid solve judges the learned one: both solve K e = f once in
+        // FP32; the learned correction stays on for this Uzawa solve only if it needs
+        // fewer flexible-CG iterations than multigrid alone
+        int rc0 = mg_setup(H);
+        if (rc0 != GG_OK) return rc0;
+        learned_prepare(H);
+        k_to_f32<<<grid_for(nd, 256), 256, 0, st>>>(nd, f, H.r32.as<float>());
+        int it_mg = 0, it_nn = 0;
+        rc0 = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), 1e-4, maxit, &it_mg,
+                      [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+        if (rc0 != GG_OK) return rc0;
+        rc0 = run_fcg(H, "fcg_nn", H.r32.as<float>(), H.e32.as<float>(), 1e-4, std::min(maxit, 40), &it_nn,
+                      [&](const float* rr, float* zz, const int32_t* dn) {
+                          vcycle(H, 0, rr, zz, dn);
+                          learned_correction(H, rr, zz, dn);
+                      });
+        H.calib_mg = it_mg;
+        H.calib_nn = it_nn;
+        S.inner_iterations += it_mg + it_nn;  // the calibration is work of this solve
+        if (rc0 != GG_OK || it_nn >= it_mg) {
+            H.nn_enabled = false;
+            H.fallbacks++;
+        }
+    }
     // STEP 1 (:553-565)
-    if ((rc = inner(f, vstar, prm.tolerance)) != GG_OK) return rc;
+    if ((rc = inner(f, vstar, prm.tolerance)) != GG_OK) return fail("first inner solve (K u* = f)", rc);
     apply_GT(H, vstar, qtmp, st);
     axpby(H, ne, -1.0, hv, 1.0, qtmp);
     const double inner_rtol = prm.inner_rtol_factor * prm.tolerance;
@@ -672,7 +727,7 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     // STEP 3 (:616-659)
     apply_G(H, q, ftmp, st);
     axpby(H, nd, 1.0, f, -1.0, ftmp);
-    if ((rc = inner(ftmp, u, inner_rtol)) != GG_OK) return rc;
+    if ((rc = inner(ftmp, u, inner_rtol)) != GG_OK) return fail("velocity solve K u = f - G p", rc);
     apply_GT(H, u, r, st);
     axpby(H, ne, -1.0, hv, 1.0, r);
     // STEP 4 (:664-837)
@@ -690,19 +745,29 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
         else
             axpby(H, ne, 1.0, qtmp, zr / zr_prev, s);
         apply_G(H, s, ftmp, st);
-        if ((rc = inner(ftmp, vstar, inner_rtol)) != GG_OK) return rc;
+        // recycling (fast path only): s = z + β s_prev, so β u*_prev = K⁻¹ G (β s_prev)
+        // is a start for K u* = G s that leaves only K⁻¹ G z to find; the stopping rule
+        // stays relative to ‖G s‖
+        const bool warm = prm.recycle_directions && prm.precision == GG_PRECISION_MIXED && it > 0;
+        if (warm) axpby(H, nd, 0.0, vstar, zr / zr_prev, vstar);
+        if ((rc = inner(ftmp, vstar, inner_rtol, warm)) != GG_OK) return fail("inner solve K u* = G s", rc);
         apply_GT(H, vstar, qtmp, st);
         const double sq = dot(H, ne, s, qtmp);
         const double alpha = zr / sq;
-        if (!isfinite(zr) || !isfinite(sq) || !isfinite(alpha)) return GG_ERR_NONFINITE;
+        if (!isfinite(zr) || !isfinite(sq) || !isfinite(alpha)) return fail("conjugate-direction step", GG_ERR_NONFINITE);
         axpby(H, ne, alpha, s, 1.0, q);
         axpby(H, nd, -alpha, vstar, 1.0, u);
         axpby(H, ne, -alpha, qtmp, 1.0, r);
         zr_prev = zr;
         absres = sqrt(dot(H, ne, r, r)) / scaleq;
         relres = absres / rhs_scale;
-        if (!isfinite(absres)) return GG_ERR_NONFINITE;
-        if (!(it < prm.max_iterations)) { rc = GG_ERR_NOT_CONVERGED; it++; break; }
+        if (!isfinite(absres)) return fail("pressure residual", GG_ERR_NONFINITE);
+        if (!(it < prm.max_iterations)) {
+            rc = GG_ERR_NOT_CONVERGED;
+            it++;
+            H.fail_where = "outer iteration limit reached";
+            break;
+        }
         it++;
         const double chosen = prm.use_absolute_tolerance ? absres : relres;
         if (!((chosen > prm.tolerance) || (it < prm.min_iterations))) break;

@@ -171,8 +171,9 @@ def Mesh(dim, elements, minCoord=None, maxCoord=None) -> abi.MeshDesc:
 def UzawaSolver(tolerance=1e-5, maxIterations=1000, minIterations=1,
                 useAbsoluteTolerance=False, preconditioner=True, inner="jacobi",
                 precision="fp64", innerRtolFactor=0.1, innerMaxIterations=10000,
-                reusePressure=False) -> abi.UzawaParams:
-    """Stokes_SLE_UzawaSolver XML parameters (Stokes_SLE_UzawaSolver.cxx:241-264)."""
+                reusePressure=False, recycle=None) -> abi.UzawaParams:
+    """Stokes_SLE_UzawaSolver XML parameters (Stokes_SLE_UzawaSolver.cxx:241-264).
+    recycle (default: on for the mixed path) starts each inner solve from β u*_prev."""
     p = abi.UzawaParams()
     p.tolerance = tolerance
     p.max_iterations = maxIterations
@@ -185,6 +186,7 @@ def UzawaSolver(tolerance=1e-5, maxIterations=1000, minIterations=1,
     p.inner_rtol_factor = innerRtolFactor
     p.inner_max_iterations = innerMaxIterations
     p.reuse_pressure = int(reusePressure)
+    p.recycle_directions = int(precision == "mixed" if recycle is None else recycle)
     return p
 
 

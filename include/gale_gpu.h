@@ -147,6 +147,9 @@ typedef struct gg_uzawa_params {
     double  inner_rtol_factor;    /* inner rtol = factor*tolerance (0.1)                */
     int32_t inner_max_iterations; /* per inner solve (PETSc default 10000)              */
     int32_t reuse_pressure;       /* start from the p passed in (Picard, restart)       */
+    int32_t recycle_directions;   /* GG_PRECISION_MIXED only: start the inner solve of
+                                     K u* = G s from β u*_prev (s = z + β s_prev); the
+                                     inner stopping rule stays relative to ‖G s‖        */
 } gg_uzawa_params;
 
 typedef struct gg_uzawa_stats {
