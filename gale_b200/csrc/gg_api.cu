@@ -102,12 +102,12 @@ void gauss_G(int dim, const double* h, double Ge[8][3]) {
     }
 }
 
+}  // namespace
+
 int set_error(Handle& H, int code, const std::string& msg) {
     H.err = msg;
     return code;
 }
-
-}  // namespace
 
 MeshK make_mesh(const gg_mesh_desc& d) {
     MeshK mk{};

@@ -349,7 +349,8 @@ int gg_learned_set_weights(gg_handle* h, int32_t level, const float* weights, in
 
 int gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const float* inputs, const float* targets,
                     const float* weights, float* outputs, float* gradient, double* loss, int32_t* grid_nodes) {
-    if (!h || batch < 1 || !inputs || !targets || !weights || !outputs || !gradient || !loss) return GG_ERR_INVALID;
+    if (!h || batch < 1 || !inputs || !targets || !weights || !outputs || !gradient || !loss || !grid_nodes)
+        return GG_ERR_INVALID;
     Handle& H = h->H;
     if (!H.built || H.built_precision != GG_PRECISION_MIXED)
         return gg::err(H, GG_ERR_STATE, "needs an operator built with GG_PRECISION_MIXED");
@@ -357,8 +358,14 @@ int gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const float* inp
     GG_TRY2(h, {
         rc = gg::learned_set_level(H, level);
         if (rc == GG_OK) {
-            if (grid_nodes) *grid_nodes = (int32_t)H.mg[H.nn_level]->nnode;
-            rc = gg::learned_eval(H, batch, inputs, targets, weights, outputs, gradient, loss);
+            const int32_t nodes = (int32_t)H.mg[H.nn_level]->nnode;
+            if (*grid_nodes != nodes) {
+                rc = gg::err(H, GG_ERR_INVALID, "buffers hold " + std::to_string(*grid_nodes) + " nodes, level " +
+                                                    std::to_string(H.nn_level) + " has " + std::to_string(nodes));
+            } else {
+                rc = gg::learned_eval(H, batch, inputs, targets, weights, outputs, gradient, loss);
+            }
+            *grid_nodes = nodes;
         }
     })
     return rc;

@@ -1,0 +1,627 @@
+// gg_fused.cu -- the multigrid-preconditioned flexible CG of the inner velocity solve as
+// ONE persistent kernel on sm_100a.
+//
+// The graph-captured solver (run_fcg in gg_solve.cu around vcycle in gg_mg.cu) issues
+// about a hundred kernels per iteration, and on the coarse levels each does a few
+// microseconds of work, so kernel boundaries set the pace.  Here one cooperative launch
+// runs a whole FP32 solve.  The phases of an iteration are:
+//   fine apply → update → (V-cycle: smoothing, restriction, dense coarse solve,
+//   prolongation on every level) → dot products → direction
+// Each phase boundary is a grid barrier instead of a kernel boundary.  The host writes the
+// phase list of one iteration (a "program" for the level hierarchy at hand) into a table
+// in device memory; the kernel copies it to shared memory and runs it with one switch, so
+// each phase body, the element apply above all, is compiled once.  Neighbouring node-wise
+// phases are fused:
+//   * the update with the level-0 Chebyshev start;
+//   * the last smoothing step with the FCG dot products;
+//   * the restriction with the coarse Chebyshev start.
+// The per-phase arithmetic is that of the separate kernels, so the iterates are those of
+// run_fcg up to the order of FP32 atomic sums.
+//
+// Grid barrier: an arrival counter in device memory; thread 0 of each block polls it with
+// an iteration limit.  When the limit expires it raises an error word; every block then
+// leaves at its next barrier, and the host reads failed = 4 (GG_ERR_CUDA).  The launch is cooperative, so the driver either makes every
+// block co-resident or refuses the launch.
+// Global reductions: each block writes one FP64 partial; after the barrier every block
+// sums all partials in block order.  Every block then holds the same value and takes the
+// same branch without a second barrier.
+// Vectors written inside the launch are read through L2 only (__ldcg): the L1 and
+// non-coherent paths are not kept coherent across blocks within a kernel.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+#include "gg_ops.cuh"
+
+namespace gg {
+
+namespace {
+
+constexpr int kFusedMaxLevels = 8;
+constexpr int kFusedBlock = 256;
+// a barrier gives up after this many polls (each an L2 round trip): a few seconds, where a
+// healthy phase takes microseconds to a millisecond
+constexpr long long kBarrierSpinLimit = 1ll << 22;
+
+struct FusedLevel {
+    MeshK mk;
+    const float* mom;
+    const uint8_t* bc;
+    const float* invd;
+    float* b;
+    float* x;
+    float* r;
+    float* d;
+    float* t;
+    float inv_theta;
+    float c1[4], c2[4];
+};
+
+// Phase types of the program.  Level 0's x and b are the FCG's z and r.
+enum : uint8_t {
+    PH_APPLY = 0,      // t_l += A_l d_l (flag 0) or A_l x_l (flag 1)
+    PH_STEP = 1,       // Chebyshev step k on level l
+    PH_STEP_DOTS = 2,  // the last level-0 step, with the partials of r·z and z·Ap
+    PH_RESTRICT = 3,   // b_{l+1} = Pᵀ(r − t)_l, Chebyshev start on l+1 when flag
+    PH_DENSE = 4,      // x_l = A_l⁻¹ b_l (coarsest level)
+    PH_PROLONG = 5,    // x_l += P x_{l+1}, t_l = 0
+    PH_RESTART = 6,    // post-smoothing start on level l
+    PH_DIR = 7,        // FCG: p = z + βp, Ap = 0
+    PH_APPLY_P = 8,    // FCG: Ap = K p with the partials of pᵀAp
+    PH_UPDATE = 9,     // FCG: x += αp, r −= αAp, ‖r‖² partials, level-0 Chebyshev start
+};
+
+struct FusedPhase {
+    uint8_t type, level, k, flag;
+};
+
+constexpr int kMaxPhases = 128;
+
+struct FusedTable {
+    int nlevels;   // levels 0..nlevels-1; the last one is solved by the dense inverse
+    int nphase;    // phases of one iteration
+    int coarse_n;
+    int pad;
+    const float* coarse_inv;
+    FusedLevel lv[kFusedMaxLevels];
+    FusedPhase ph[kMaxPhases];
+};
+
+constexpr int kTabWords = (int)((sizeof(FusedTable) + 15) / 16);
+
+struct GridBarrier {
+    unsigned int arrive;  // arrivals since the launch (zeroed by the host before it)
+    unsigned int pad0;
+    int err;              // set by a block whose wait gave up
+    int pad1;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// All blocks of the grid meet here.  Arrival is a release reduction on a counter that only
+// grows (barrier e of the launch completes when it reaches e·gridDim.x); waiting is an
+// acquire poll of that counter.  The release/acquire pair orders every write of the block
+// (made visible to thread 0 by __syncthreads) before every read after the barrier.
+// Returns false (uniformly within the block) once any block has given up waiting; the
+// caller then leaves the kernel.
+__device__ __noinline__ bool grid_barrier(GridBarrier* gb, unsigned int* epoch) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int target = (*epoch + 1) * gridDim.x;
+        int ok = 1;
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&gb->arrive), "r"(1u) : "memory");
+        long long spins = 0;
+        while (ld_acquire_gpu(&gb->arrive) < target) {
+            if (++spins > kBarrierSpinLimit || ((spins & 1023) == 0 && *(volatile int*)&gb->err)) {
+                atomicExch(&gb->err, 1);
+                ok = 0;
+                break;
+            }
+        }
+        s_ok = ok;
+        *epoch = *epoch + 1;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ void put_partial(double v, double* slot) {
+    v = block_sum(v);
+    if (threadIdx.x == 0) __stcg(&slot[blockIdx.x], v);
+}
+
+// Σ of the per-block partials in block order; identical in every block.
+__device__ __noinline__ double all_sum(const double* slot) {
+    __shared__ double s_val;
+    double v = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) v += __ldcg(&slot[b]);
+    v = block_sum(v);
+    if (threadIdx.x == 0) s_val = v;
+    __syncthreads();
+    v = s_val;
+    __syncthreads();
+    return v;
+}
+
+__device__ __forceinline__ int64_t gtid() { return blockIdx.x * (int64_t)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * blockDim.x; }
+
+// t += A v on level L (element tiles block-strided); returns this thread's Σ v_eᵀ A_e v_e
+// when kEnergy
+template <int DIM, bool kEnergy>
+__device__ __forceinline__ double phase_apply(const FusedLevel& L, const float* v, float* t) {
+    return apply_tiles<DIM, float, 1, kEnergy>(L.mk, L.mom, L.bc, v, t, blockIdx.x, gridDim.x);
+}
+
+// r −= t, d = c1 d + c2 D⁻¹ r, x += d, t = 0
+template <int DIM>
+__device__ __forceinline__ void phase_cheb_step(const FusedLevel& L, int k) {
+    const int64_t n = (int64_t)DIM * L.mk.nnode;
+    const float c1 = L.c1[k], c2 = L.c2[k];
+    float* xl = L.x;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float rv = __ldcg(&L.r[i]) - __ldcg(&L.t[i]);
+        const float dv = c1 * __ldcg(&L.d[i]) + c2 * L.invd[i] * rv;
+        L.r[i] = rv;
+        L.d[i] = dv;
+        xl[i] = __ldcg(&xl[i]) + dv;
+        L.t[i] = 0.f;
+    }
+}
+
+// the same step on level 0, finishing z, with the FCG partial sums r·z and z·Ap
+template <int DIM>
+__device__ __forceinline__ void phase_cheb_step_dots(const FusedLevel& L, int k, const float* Ap, double& rz,
+                                                     double& zap) {
+    const int64_t n = (int64_t)DIM * L.mk.nnode;
+    const float c1 = L.c1[k], c2 = L.c2[k];
+    float* z = L.x;
+    const float* rf = L.b;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float rv = __ldcg(&L.r[i]) - __ldcg(&L.t[i]);
+        const float dv = c1 * __ldcg(&L.d[i]) + c2 * L.invd[i] * rv;
+        L.r[i] = rv;
+        L.d[i] = dv;
+        const float zv = __ldcg(&z[i]) + dv;
+        z[i] = zv;
+        L.t[i] = 0.f;
+        rz += (double)__ldcg(&rf[i]) * (double)zv;
+        zap += (double)zv * (double)__ldcg(&Ap[i]);
+    }
+}
+
+// post-smoothing start from x: r = b − t (t = A x), d = D⁻¹r/θ, x += d, t = 0
+template <int DIM>
+__device__ __forceinline__ void phase_restart(const FusedLevel& L) {
+    const int64_t n = (int64_t)DIM * L.mk.nnode;
+    const float* bl = L.b;
+    float* xl = L.x;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float rv = __ldcg(&bl[i]) - __ldcg(&L.t[i]);
+        const float dv = L.inv_theta * L.invd[i] * rv;
+        L.r[i] = rv;
+        L.d[i] = dv;
+        xl[i] = __ldcg(&xl[i]) + dv;
+        L.t[i] = 0.f;
+    }
+}
+
+// b_C = Pᵀ (r − t)_L (zero on coarse BC dofs); when C is smoothed, its Chebyshev start:
+// r = b, d = D⁻¹b/θ, x = d, t = 0
+template <int DIM>
+__device__ __forceinline__ void phase_restrict(const FusedLevel& L, const FusedLevel& C, bool start) {
+    const MeshK& fk = L.mk;
+    const MeshK& ck = C.mk;
+    for (int64_t N = gtid(); N < ck.nnode; N += gstride()) {
+        const int I = (int)(N % ck.nn[0]);
+        const int64_t rr = N / ck.nn[0];
+        const int J = (int)(rr % ck.nn[1]), K = DIM == 3 ? (int)(rr / ck.nn[1]) : 0;
+        float acc[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) acc[c] = 0.f;
+#pragma unroll
+        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); dz++)
+#pragma unroll
+            for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
+                    if (i < 0 || j < 0 || k < 0 || i >= fk.nn[0] || j >= fk.nn[1] || k >= fk.nn[2]) continue;
+                    const float w = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+                    const int64_t n = i + (int64_t)fk.nn[0] * (j + (int64_t)fk.nn[1] * k);
+#pragma unroll
+                    for (int c = 0; c < DIM; c++) {
+                        const int64_t q = (int64_t)c * fk.nnode + n;
+                        acc[c] += w * (__ldcg(&L.r[q]) - __ldcg(&L.t[q]));
+                    }
+                }
+        const uint8_t bm = C.bc[N];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) {
+            const int64_t q = (int64_t)c * ck.nnode + N;
+            const float bv = ((bm >> c) & 1) ? 0.f : acc[c];
+            C.b[q] = bv;
+            if (start) {
+                const float dv = C.inv_theta * C.invd[q] * bv;
+                C.r[q] = bv;
+                C.d[q] = dv;
+                C.x[q] = dv;
+                C.t[q] = 0.f;
+            }
+        }
+    }
+}
+
+// x_L += P x_C (fine BC dofs untouched), t_L = 0
+template <int DIM>
+__device__ __forceinline__ void phase_prolong(const FusedLevel& L, const FusedLevel& C) {
+    float* xl = L.x;
+    const MeshK& fk = L.mk;
+    const MeshK& ck = C.mk;
+    for (int64_t n = gtid(); n < fk.nnode; n += gstride()) {
+        const int i = (int)(n % fk.nn[0]);
+        const int64_t rr = n / fk.nn[0];
+        const int j = (int)(rr % fk.nn[1]), k = DIM == 3 ? (int)(rr / fk.nn[1]) : 0;
+        const int idx[3] = {i, j, k};
+        int lo[3], hi[3];
+        float wl[3], wh[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (d >= DIM || (idx[d] & 1) == 0) {
+                lo[d] = hi[d] = idx[d] >> 1;
+                wl[d] = 1.f;
+                wh[d] = 0.f;
+            } else {
+                lo[d] = idx[d] >> 1;
+                hi[d] = lo[d] + 1;
+                wl[d] = wh[d] = 0.5f;
+            }
+        }
+        float acc[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) acc[c] = 0.f;
+#pragma unroll
+        for (int q = 0; q < (1 << DIM); q++) {
+            const int I = (q & 1) ? hi[0] : lo[0], J = (q & 2) ? hi[1] : lo[1], K = (q & 4) ? hi[2] : lo[2];
+            const float w = ((q & 1) ? wh[0] : wl[0]) * ((q & 2) ? wh[1] : wl[1]) *
+                            (DIM == 3 ? ((q & 4) ? wh[2] : wl[2]) : 1.f);
+            if (w == 0.f) continue;
+            const int64_t N = I + (int64_t)ck.nn[0] * (J + (int64_t)ck.nn[1] * K);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) acc[c] += w * __ldcg(&C.x[(int64_t)c * ck.nnode + N]);
+        }
+        const uint8_t bm = L.bc[n];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) {
+            const int64_t q = (int64_t)c * fk.nnode + n;
+            if (!((bm >> c) & 1)) xl[q] = __ldcg(&xl[q]) + acc[c];
+            L.t[q] = 0.f;
+        }
+    }
+}
+
+// x = A⁻¹ b on the coarsest level: one warp per row of the dense FP32 inverse
+__device__ __forceinline__ void phase_dense(int n, const float* A, const float* b, float* x) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t row = gtid() >> 5; row < n; row += gstride() >> 5) {
+        float s = 0.f;
+        for (int k = lane; k < n; k += 32) s += A[row * n + k] * __ldcg(&b[k]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) x[row] = s;
+    }
+}
+
+// x = 0, r = b (BC rows zero), p = Ap = 0 (update = false); or x += αp, r −= αAp
+// (update = true); then the level-0 Chebyshev start on r.  Returns this thread's Σ r².
+template <int DIM>
+__device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool update, float alpha, const float* b,
+                                                     float* x, float* p, float* Ap) {
+    const int64_t nnode = L0.mk.nnode, n = (int64_t)DIM * nnode;
+    float* r = L0.b;
+    float* z = L0.x;
+    double acc = 0.0;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        float rv;
+        if (update) {
+            x[i] = __ldcg(&x[i]) + alpha * __ldcg(&p[i]);
+            rv = __ldcg(&r[i]) - alpha * __ldcg(&Ap[i]);  // BC rows of Ap are zero
+        } else {
+            const int c = (int)(i / nnode);
+            const bool fixed = (L0.bc[i - (int64_t)c * nnode] >> c) & 1;
+            rv = fixed ? 0.f : b[i];
+            x[i] = 0.f;
+            p[i] = 0.f;
+            Ap[i] = 0.f;
+        }
+        r[i] = rv;
+        acc += (double)rv * (double)rv;
+        const float dv = L0.inv_theta * L0.invd[i] * rv;
+        L0.r[i] = rv;
+        L0.d[i] = dv;
+        z[i] = dv;
+        L0.t[i] = 0.f;
+    }
+    return acc;
+}
+
+// The whole solve; returns false if a barrier gave up.
+template <int DIM>
+__device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, float* x, float* p, float* Ap,
+                                         double rtol, int maxit, KrylovScalars* ks, double* part, GridBarrier* gb) {
+    const FusedLevel& L0 = T.lv[0];
+    const int64_t n = (int64_t)DIM * L0.mk.nnode;
+    const int G = gridDim.x;
+    double* p_rr = part;
+    double* p_rz = part + G;
+    double* p_zap = part + 2 * G;
+    double* p_pap = part + 3 * G;
+    unsigned int epoch = 0;
+    put_partial(phase_update_start<DIM>(L0, false, 0.f, b, x, p, Ap), p_rr);
+    if (!grid_barrier(gb, &epoch)) return false;
+    const double rnorm0 = sqrt(all_sum(p_rr));
+    const double tt = rtol * rnorm0;
+    const double ttol = tt < 1e-30 ? 1e-30 : tt;
+    double rn = rnorm0, rz = 0.0, pAp = 1.0;
+    float alpha = 0.f, beta = 0.f;
+    int it = 0, failed = 0;
+    bool done = rnorm0 <= ttol;
+    while (!done) {
+        for (int q = 0; q < T.nphase && !done; q++) {
+            const FusedPhase P = T.ph[q];
+            const FusedLevel& L = T.lv[P.level];
+            switch (P.type) {
+                case PH_APPLY:
+                    phase_apply<DIM, false>(L, P.flag ? L.x : L.d, L.t);
+                    break;
+                case PH_APPLY_P:
+                    put_partial(phase_apply<DIM, true>(L0, p, Ap), p_pap);
+                    break;
+                case PH_STEP:
+                    phase_cheb_step<DIM>(L, P.k);
+                    break;
+                case PH_STEP_DOTS: {
+                    double rzp = 0.0, zap = 0.0;
+                    phase_cheb_step_dots<DIM>(L, P.k, Ap, rzp, zap);
+                    put_partial(rzp, p_rz);
+                    put_partial(zap, p_zap);
+                    break;
+                }
+                case PH_RESTRICT:
+                    phase_restrict<DIM>(L, T.lv[P.level + 1], P.flag != 0);
+                    break;
+                case PH_DENSE:
+                    phase_dense(T.coarse_n, T.coarse_inv, L.b, L.x);
+                    break;
+                case PH_PROLONG:
+                    phase_prolong<DIM>(L, T.lv[P.level + 1]);
+                    break;
+                case PH_RESTART:
+                    phase_restart<DIM>(L);
+                    break;
+                case PH_DIR:
+                    for (int64_t i = gtid(); i < n; i += gstride()) {
+                        p[i] = __ldcg(&L0.x[i]) + beta * __ldcg(&p[i]);
+                        Ap[i] = 0.f;
+                    }
+                    break;
+                case PH_UPDATE:
+                    put_partial(phase_update_start<DIM>(L0, true, alpha, b, x, p, Ap), p_rr);
+                    break;
+                default:
+                    break;
+            }
+            if (!grid_barrier(gb, &epoch)) return false;
+            // scalars after the phases that end in a reduction (same value in every block)
+            if (P.type == PH_STEP_DOTS) {
+                rz = all_sum(p_rz);
+                const double zap = all_sum(p_zap);
+                // truncated flexible CG (Notay 2000): β = −(z·Ap)/(pᵀAp), p = z on the first step
+                beta = it == 0 ? 0.f : (float)(-zap / pAp);
+            } else if (P.type == PH_APPLY_P) {
+                pAp = all_sum(p_pap);
+                if (!(pAp > 0.0) || isinf(pAp)) {
+                    failed = 3;
+                    done = true;
+                } else {
+                    alpha = (float)(rz / pAp);
+                }
+            } else if (P.type == PH_UPDATE) {
+                rn = sqrt(all_sum(p_rr));
+                it++;
+                if (!(rn == rn) || isinf(rn)) {
+                    failed = 2;
+                    done = true;
+                } else if (rn <= ttol) {
+                    done = true;
+                } else if (it >= maxit) {
+                    failed = 1;
+                    done = true;
+                }
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ks->rnorm0 = rnorm0;
+        ks->rnorm = rn;
+        ks->ttol = ttol;
+        ks->rz = rz;
+        ks->pAp = pAp;
+        ks->iterations = it;
+        ks->failed = failed;
+        ks->maxit = maxit;
+        ks->done = 1;
+    }
+    return true;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kFusedBlock, 2)
+k_fcg_fused(const int4* __restrict__ tab, const float* __restrict__ b, float* x, float* p, float* Ap, double rtol,
+            int maxit, KrylovScalars* ks, double* part, GridBarrier* gb) {
+    __shared__ int4 s_tab[kTabWords];
+    for (int i = threadIdx.x; i < kTabWords; i += blockDim.x) s_tab[i] = tab[i];
+    __syncthreads();
+    const FusedTable& T = *reinterpret_cast<const FusedTable*>(s_tab);
+    if (!fcg_body<DIM>(T, b, x, p, Ap, rtol, maxit, ks, part, gb) && threadIdx.x == 0) {
+        ks->failed = 4;
+        ks->done = 1;
+    }
+}
+
+struct FusedLaunch {
+    int max_blocks[4] = {0, 0, 0, 0};  // co-resident blocks per device, by DIM
+    bool probed[4] = {false, false, false, false};
+};
+
+}  // namespace
+
+// On unless the environment sets GALE_B200_FUSED_FCG=0, which selects the graph-captured
+// kernel sequence (read at every solve, so one process can compare both).
+bool fused_fcg_enabled() {
+    const char* e = getenv("GALE_B200_FUSED_FCG");
+    return !(e && e[0] == '0');
+}
+
+// Multigrid FCG in one cooperative launch: x = K32⁻¹ b to ‖r‖ ≤ rtol‖b‖.  Returns
+// GG_OK / GG_ERR_NOT_CONVERGED / GG_ERR_NONFINITE / GG_ERR_CUDA, or 1 when the hierarchy
+// does not fit this kernel (the caller then runs the graph-captured solver).
+int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters) {
+    const size_t nl = H.mg.size();
+    const int deg = H.mg_degree;
+    if (nl < 2 || nl > (size_t)kFusedMaxLevels || !H.coarse_n || deg < 2 || deg > 4) return 1;
+    const int dim = H.dim;
+    static std::mutex mu;
+    static FusedLaunch fl[16];
+    int dev = 0;
+    GG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16) return 1;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        FusedLaunch& f = fl[dev];
+        if (!f.probed[dim]) {
+            int coop = 0;
+            GG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+            int per_sm = 0;
+            if (coop) {
+                if (dim == 2)
+                    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fcg_fused<2>, kFusedBlock, 0));
+                else
+                    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fcg_fused<3>, kFusedBlock, 0));
+            }
+            f.max_blocks[dim] = per_sm * num_sms();
+            f.probed[dim] = true;
+        }
+        if (f.max_blocks[dim] <= 0) return 1;
+    }
+    const int max_blocks = fl[dev].max_blocks[dim];
+    float* r = H.cgr32.as<float>();
+    float* z = H.z32.as<float>();
+    if (H.fused_gen != H.mg_gen || H.fused_r != r || H.fused_z != z) {
+        FusedTable T;
+        std::memset(&T, 0, sizeof T);
+        T.nlevels = (int)nl;
+        T.coarse_n = (int)H.coarse_n;
+        T.coarse_inv = H.coarse_inv.as<float>();
+        for (size_t l = 0; l < nl; l++) {
+            const MGLevel& L = *H.mg[l];
+            FusedLevel& F = T.lv[l];
+            F.mk = L.mk;
+            F.mom = L.mom32;
+            F.bc = L.bcmask;
+            F.invd = L.invdiag.as<float>();
+            F.b = l == 0 ? r : L.b.as<float>();  // level 0 smooths the FCG residual into z
+            F.x = l == 0 ? z : L.x.as<float>();
+            F.r = L.r.as<float>();
+            F.d = L.d.as<float>();
+            F.t = L.t.as<float>();
+            const ChebCoef cc = cheb_coef(L.lambda_max, deg);
+            F.inv_theta = cc.inv_theta;
+            for (int k = 0; k < 4; k++) {
+                F.c1[k] = cc.c1[k];
+                F.c2[k] = cc.c2[k];
+            }
+        }
+        // one iteration: the V-cycle after the level-0 start (which PH_UPDATE performs),
+        // then direction, apply and update
+        std::vector<FusedPhase> prog;
+        auto ph = [&](uint8_t type, int level, int k = 0, int flag = 0) {
+            prog.push_back(FusedPhase{type, (uint8_t)level, (uint8_t)k, (uint8_t)flag});
+        };
+        const int ns = (int)nl - 1;  // smoothed levels
+        for (int l = 0; l < ns; l++) {
+            for (int k = 1; k < deg; k++) {
+                ph(PH_APPLY, l, 0, 0);
+                ph(PH_STEP, l, k);
+            }
+            ph(PH_APPLY, l, 0, 0);
+            ph(PH_RESTRICT, l, 0, l + 1 < ns ? 1 : 0);
+        }
+        ph(PH_DENSE, ns);
+        for (int l = ns - 1; l >= 0; l--) {
+            ph(PH_PROLONG, l);
+            ph(PH_APPLY, l, 0, 1);
+            ph(PH_RESTART, l);
+            for (int k = 1; k < deg; k++) {
+                ph(PH_APPLY, l, 0, 0);
+                ph(l == 0 && k == deg - 1 ? PH_STEP_DOTS : PH_STEP, l, k);
+            }
+        }
+        ph(PH_DIR, 0);
+        ph(PH_APPLY_P, 0);
+        ph(PH_UPDATE, 0);
+        if ((int)prog.size() > kMaxPhases) return 1;
+        T.nphase = (int)prog.size();
+        for (size_t q = 0; q < prog.size(); q++) T.ph[q] = prog[q];
+        H.fused_host.assign(kTabWords * 16, 0);
+        std::memcpy(H.fused_host.data(), &T, sizeof T);
+        H.fused_tab.ensure(kTabWords * 16);
+        GG_CUDA(cudaMemcpyAsync(H.fused_tab.p, H.fused_host.data(), kTabWords * 16, cudaMemcpyHostToDevice, H.stream));
+        H.fused_gen = H.mg_gen;
+        H.fused_r = r;
+        H.fused_z = z;
+        H.fused_phases = T.nphase;
+    }
+    const int64_t n = H.ndof;
+    int grid = (int)std::min<int64_t>((int64_t)max_blocks, (n + kFusedBlock - 1) / kFusedBlock);
+    if (grid < 1) grid = 1;
+    // the barrier counter reaches (barriers of the launch) × grid: keep it inside 32 bits
+    if ((double)(maxit + 2) * (H.fused_phases + 1) * grid >= 2147483648.0) return 1;
+    H.fused_part.ensure(sizeof(double) * 4 * grid);
+    H.fused_bar.ensure(sizeof(GridBarrier));
+    GG_CUDA(cudaMemsetAsync(H.fused_bar.p, 0, sizeof(GridBarrier), H.stream));
+    const int4* tab = H.fused_tab.as<int4>();
+    float* p = H.p32.as<float>();
+    float* Ap = H.Ap32.as<float>();
+    KrylovScalars* ks = H.scal.as<KrylovScalars>();
+    double* part = H.fused_part.as<double>();
+    GridBarrier* gb = H.fused_bar.as<GridBarrier>();
+    void* args[] = {(void*)&tab, (void*)&b,      (void*)&x,   (void*)&p,    (void*)&Ap, (void*)&rtol,
+                    (void*)&maxit, (void*)&ks, (void*)&part, (void*)&gb};
+    const void* fn = dim == 2 ? (const void*)k_fcg_fused<2> : (const void*)k_fcg_fused<3>;
+    GG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kFusedBlock), args, 0, H.stream));
+    H.kernel_launches += 1;
+    GG_CUDA(cudaMemcpyAsync(H.h_scal, ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, H.stream));
+    GG_CUDA(cudaStreamSynchronize(H.stream));
+    *iters = H.h_scal->iterations;
+    if (H.h_scal->failed == 4) {
+        H.err = "fused multigrid solve: grid barrier timed out";
+        return GG_ERR_CUDA;
+    }
+    if (H.h_scal->failed == 1) return GG_ERR_NOT_CONVERGED;
+    if (H.h_scal->failed) return GG_ERR_NONFINITE;
+    return GG_OK;
+}
+
+}  // namespace gg

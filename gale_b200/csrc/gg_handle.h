@@ -102,6 +102,13 @@ struct Handle {
     DBuf mg_part, mg_dense; // power-iteration partials; FP64 columns of the coarsest operator
     int64_t coarse_n = 0;   // 0: no dense coarse solve (Chebyshev on the coarsest level)
     int mg_degree = 2;      // Chebyshev degree of the smoother
+    // persistent multigrid FCG (gg_fused.cu): level table for the current hierarchy
+    DBuf fused_tab, fused_part, fused_bar;
+    std::vector<unsigned char> fused_host;
+    int64_t fused_gen = -2;  // mg_gen the table was written for
+    const float* fused_r = nullptr;  // FCG residual / preconditioned vector baked into it
+    const float* fused_z = nullptr;
+    int fused_phases = 0;            // grid barriers per iteration
     // learned coarse correction (gg_learned.cu)
     std::shared_ptr<struct LearnedState> learned;
     bool nn_ready = false;

@@ -9,6 +9,8 @@ namespace gg {
 
 int num_sms();
 int grid_for(int64_t n, int block);
+// Record a message for gg_last_error and return the status code (gg_api.cu).
+int set_error(Handle& H, int code, const std::string& msg);
 
 // Vertex coordinate, CartesianGenerator_CalcGeom (StgDomain/Mesh/src/
 // CartesianGenerator.cxx:2178-2215), with explicit roundings (no FMA contraction).
@@ -58,12 +60,23 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
 void release_graphs(Handle& H);
 
 // Multigrid (gg_mg.cu): hierarchy for the current build; z = M⁻¹ b on level l.
+// Chebyshev–Jacobi smoother of degree `degree` on [0.1, 1.1]·λ_max(D⁻¹A):
+// x₀ = D⁻¹r/θ, then d_k = c1[k] d_{k−1} + c2[k] D⁻¹ r_k.
+struct ChebCoef {
+    float inv_theta;
+    float c1[8], c2[8];
+};
+ChebCoef cheb_coef(double lmax_est, int degree);
 int mg_setup(Handle& H);
 void vcycle(Handle& H, size_t l, const float* b, float* x, const int32_t* done);
 void mg_restrict(Handle& H, size_t l, const float* fine, float* coarse, const int32_t* done);
 void mg_prolong_add(Handle& H, size_t l, const float* coarse, float* fine, const int32_t* done);
 // x = K32⁻¹ b by the multigrid flexible CG (FP32, ‖r‖ ≤ rtol‖b‖)
 int fcg_mg_solve(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters);
+// The same solve as one persistent cooperative kernel (gg_fused.cu); returns 1 when the
+// hierarchy does not fit it (no dense coarse level, > 8 levels, degree outside 2..4).
+int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters);
+bool fused_fcg_enabled();
 
 // Learned coarse correction (gg_learned.cu)
 bool learned_ready(Handle& H);

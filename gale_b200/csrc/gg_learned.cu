@@ -496,8 +496,11 @@ static void init_weights(Handle& H, uint64_t seed) {
 int learned_set_level(Handle& H, int level) {
     int rc = mg_setup(H);
     if (rc != GG_OK) return rc;
-    if (H.mg.size() < 2) return GG_ERR_INVALID;
-    size_t L = level <= 0 ? std::min<size_t>(2, H.mg.size() - 1) : std::min<size_t>(level, H.mg.size() - 1);
+    if (H.mg.size() < 2) return set_error(H, GG_ERR_INVALID, "the multigrid hierarchy has a single level");
+    if (level >= (int)H.mg.size())
+        return set_error(H, GG_ERR_INVALID, "learned level " + std::to_string(level) + " does not exist (levels 1.." +
+                                                std::to_string(H.mg.size() - 1) + ")");
+    size_t L = level <= 0 ? std::min<size_t>(2, H.mg.size() - 1) : (size_t)level;
     if (!H.learned || learned(H).level != L || learned(H).w32.p == nullptr) ensure_net(H, L);
     H.nn_level = (int)L;
     return GG_OK;

@@ -31,7 +31,8 @@ MeshK make_mesh(const gg_mesh_desc& d);
 
 namespace {
 
-constexpr int kMinCoarse = 4;  // coarsen while every axis is even and ≥ 4 elements
+constexpr int kMinCoarse = 4;      // coarsen while every axis is even and ≥ 4 elements
+constexpr int64_t kDenseStop = 1000;  // … and the level has more dofs than this
 
 __device__ __forceinline__ double tcoef(int a, int ap, double o) {
     // ξ_c = (ξ_f + o)/2  ⇒  ξ_c^a = Σ_{a'≤a} T[a][a'] ξ_f^{a'}
@@ -337,10 +338,7 @@ __global__ void k_unit(int64_t n, int64_t j, double* __restrict__ x) {
 
 int g(int64_t n) { return grid_for(n, 256); }
 
-struct ChebCoef {
-    float inv_theta;
-    float c1[8], c2[8];
-};
+}  // namespace
 
 ChebCoef cheb_coef(double lmax_est, int degree) {
     const double lmax = 1.1 * lmax_est, lmin = 0.1 * lmax_est;
@@ -357,8 +355,6 @@ ChebCoef cheb_coef(double lmax_est, int degree) {
     }
     return cc;
 }
-
-}  // namespace
 
 // Enqueue the V-cycle z = M⁻¹ b on level l (b and x are level-l vectors).
 void vcycle(Handle& H, size_t l, const float* b, float* x, const int32_t* done) {
@@ -531,6 +527,8 @@ int mg_setup(Handle& H) {
         H.mg.push_back(std::move(L0));
         for (;;) {
             const MeshK& f = H.mg.back()->mk;
+            // a level small enough for the dense coarse inverse ends the hierarchy
+            if (H.mg.size() > 1 && f.nnode * dim <= kDenseStop) break;
             bool can = true;
             for (int d = 0; d < dim; d++)
                 if (f.n[d] % 2 != 0 || f.n[d] < kMinCoarse) can = false;

@@ -1,7 +1,8 @@
 // gg_ops.cu -- matrix-free K, G and Gᵀ on sm_100a.
 //
 // K apply (replaces MatMult with the assembled k_matrix of __StiffnessMatrix_NewAssemble,
-// StgFEM/SLE/SystemSetup/src/StiffnessMatrix.cxx:2016-2200).  One thread per element:
+// StgFEM/SLE/SystemSetup/src/StiffnessMatrix.cxx:2016-2200).  One thread per element, a
+// block per tile of 32×4×2 elements (32×8 in 2D), x fastest:
 //   1. gather the 2^dim nodal values per component (coalesced along x),
 //   2. Walsh–Hadamard transform → modal coefficients m[c][S] = Σ_a Π_{d∈S} s_d(a) u_a,c,
 //   3. velocity gradient ∂u_c/∂x_d = κ_d Σ_{T⊆others(d)} m[c][{d}∪T] ξ^T,
@@ -16,18 +17,14 @@
 
 namespace gg {
 
-template <int DIM, typename R>
+template <int DIM, typename R, bool kEnergy>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
 k_apply_K(MeshK mk, const R* __restrict__ mom, const uint8_t* __restrict__ bcmask,
           const R* __restrict__ x, R* __restrict__ y, double* __restrict__ energy_part,
           const int32_t* __restrict__ done) {
     if (done && *done) return;
-    const int64_t nel = mk.nel;
-    double en = 0.0;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
-         e += (int64_t)gridDim.x * blockDim.x)
-        en += element_apply_scatter<DIM, R>(mk, mom, bcmask, x, y, e);
-    if (energy_part) {
+    double en = apply_tiles<DIM, R, 0, kEnergy>(mk, mom, bcmask, x, y, blockIdx.x, gridDim.x);
+    if (kEnergy) {
         en = block_sum(en);
         if (threadIdx.x == 0) energy_part[blockIdx.x] = en;
     }
@@ -36,10 +33,13 @@ k_apply_K(MeshK mk, const R* __restrict__ mom, const uint8_t* __restrict__ bcmas
 template <typename R>
 void apply_K_ex(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
                 double* energy_part, int grid, cudaStream_t st, const int32_t* done) {
-    if (mk.dim == 2)
-        k_apply_K<2, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
-    else
-        k_apply_K<3, R><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
+    if (mk.dim == 2) {
+        if (energy_part) k_apply_K<2, R, true><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
+        else k_apply_K<2, R, false><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
+    } else {
+        if (energy_part) k_apply_K<3, R, true><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
+        else k_apply_K<3, R, false><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
+    }
 }
 template void apply_K_ex<double>(const MeshK&, const double*, const uint8_t*, const double*, double*,
                                  double*, int, cudaStream_t, const int32_t*);

@@ -35,8 +35,8 @@ __device__ __forceinline__ int32_t local_node(int32_t n0, int32_t nn0, int32_t n
     return n0 + (a & 1) + ((a >> 1) & 1) * nn0 + (DIM == 3 ? ((a >> 2) & 1) * nn01 : 0);
 }
 
-// y += K_e x_e for element e, scattered with atomics to the non-BC rows; returns the
-// element energy x_eᵀ K_e x_e.
+// y += K_e x_e for element e = (i, j, k), one atomic per element node and component
+// (BC rows skipped); returns the element energy x_eᵀ K_e x_e when kEnergy (else 0).
 //
 //   m[c][S] = Σ_a Π_{d∈S} s_d(a) x_{a,c}                 (Walsh–Hadamard, in place)
 //   ∂x_c/∂x_d (ξ) = κ_d Σ_{T⊆others(d)} m[c][{d}∪T] ξ^T
@@ -47,31 +47,45 @@ __device__ __forceinline__ int32_t local_node(int32_t n0, int32_t nn0, int32_t n
 // viscosity and w·detJ inside the moments).  One output component is finished and
 // scattered before the next is formed, which keeps the live register set to the moments,
 // the modal coefficients and one component's Q.
-template <int DIM, typename R>
+// The kernel is bound by instruction issue, not by bytes (the moments and vectors of a
+// 64³ level sit in L2), so the element index arrives as (i, j, k) without divisions,
+// node addresses are corner offsets from one base, and the BC bits of the 2^dim nodes
+// are read once.
+// kLoad selects how x is read: 0 plain (may use the read-only path), 1 through L2 only
+// (ld.global.cg), 2 cached weak loads (ld.global.ca).  A persistent kernel that wrote x in
+// an earlier phase of the same launch must not use 0: the non-coherent path is only valid
+// for data that no thread writes during the kernel.
+template <int DIM, typename R, int kLoad = 0, bool kEnergy = true>
 __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R* __restrict__ mom,
                                                         const uint8_t* __restrict__ bcmask,
-                                                        const R* __restrict__ x, R* __restrict__ y,
-                                                        int64_t e) {
+                                                        const R* __restrict__ x, R* __restrict__ y, int i, int j,
+                                                        int k, int32_t e) {
     constexpr int NS = 1 << DIM;
     constexpr int NM = n_moments<DIM>();
+    const int64_t nnode = mk.nnode, nel = mk.nel;
     const int32_t nn0 = mk.nn[0], nn01 = mk.nn[0] * mk.nn[1];
-    const int32_t nnode = (int32_t)mk.nnode;
-    const int64_t nel = mk.nel;
-    const int32_t i = (int32_t)(e % mk.n[0]);
-    const int32_t r = (int32_t)(e / mk.n[0]);
-    const int32_t j = r % mk.n[1], k = r / mk.n[1];
-    const int32_t n0 = i + nn0 * (j + mk.nn[1] * k);
+    const int32_t n0 = i + nn0 * j + (DIM == 3 ? nn01 * k : 0);
+    int32_t off[NS];
+#pragma unroll
+    for (int a = 0; a < NS; a++) off[a] = (a & 1) + ((a >> 1) & 1) * nn0 + (DIM == 3 ? ((a >> 2) & 1) * nn01 : 0);
+    uint32_t fixed = 0;  // bit 4a + c: component c of corner a has a Dirichlet condition
+#pragma unroll
+    for (int a = 0; a < NS; a++) fixed |= (uint32_t)bcmask[n0 + off[a]] << (4 * a);
 
     R m[DIM][NS];
 #pragma unroll
-    for (int a = 0; a < NS; a++) {
-        const int32_t n = local_node<DIM>(n0, nn0, nn01, a);
+    for (int c = 0; c < DIM; c++) {
+        const R* xc = x + c * nnode + n0;
 #pragma unroll
-        for (int c = 0; c < DIM; c++) m[c][a] = x[(int64_t)c * nnode + n];
+        for (int a = 0; a < NS; a++) {
+            const R* px = xc + off[a];
+            m[c][a] = kLoad == 1 ? __ldcg(px) : kLoad == 2 ? __ldca(px) : *px;
+        }
     }
     R M[NM];
+    const R* Me = mom + e;
 #pragma unroll
-    for (int q = 0; q < NM; q++) M[q] = mom[(int64_t)q * nel + e];
+    for (int q = 0; q < NM; q++) M[q] = Me[q * nel];
     R kap[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; d++) kap[d] = (R)mk.kappa[d];
@@ -87,6 +101,14 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
                     m[c][a] = lo + hi;
                     m[c][a | (1 << d)] = hi - lo;
                 }
+    // velocity-gradient coefficients with κ folded in: g[c][d][T] = κ_d m[c][{d}∪T]
+    R g[DIM][DIM][NS];
+#pragma unroll
+    for (int c = 0; c < DIM; c++)
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int T = 0; T < NS; T++) g[c][d][T] = ((T >> d) & 1) ? R(0) : kap[d] * m[c][T | (1 << d)];
 
     double energy = 0.0;
 #pragma unroll
@@ -106,17 +128,19 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
                     const int e1 = ((U >> 1) & 1) + ((T >> 1) & 1);
                     const int e2 = DIM == 3 ? ((U >> 2) & 1) + ((T >> 2) & 1) : 0;
                     if (c == d) {
-                        if (!((T >> c) & 1))
-                            acc += (R(2) * kap[c] * m[c][T | (1 << c)]) * M[mom_slot<DIM>(e0, e1, e2)];
+                        if (!((T >> c) & 1)) acc += g[c][c][T] * M[mom_slot<DIM>(e0, e1, e2)];
                     } else {
-                        if (!((T >> d) & 1)) acc += (kap[d] * m[c][T | (1 << d)]) * M[mom_slot<DIM>(e0, e1, e2)];
-                        if (!((T >> c) & 1)) acc += (kap[c] * m[d][T | (1 << c)]) * M[mom_slot<DIM>(e0, e1, e2)];
+                        if (!((T >> d) & 1)) acc += g[c][d][T] * M[mom_slot<DIM>(e0, e1, e2)];
+                        if (!((T >> c) & 1)) acc += g[d][c][T] * M[mom_slot<DIM>(e0, e1, e2)];
                     }
                 }
-                Q[U | (1 << d)] += kap[d] * acc;
+                // σ_cc carries the factor 2 of D0
+                Q[U | (1 << d)] += (c == d ? R(2) * kap[d] : kap[d]) * acc;
             }
+        if (kEnergy) {
 #pragma unroll
-        for (int S = 1; S < NS; S++) energy += (double)m[c][S] * (double)Q[S];
+            for (int S = 1; S < NS; S++) energy += (double)m[c][S] * (double)Q[S];
+        }
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
@@ -126,13 +150,47 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
                     Q[a] = q0 - q1;
                     Q[a | (1 << d)] = q0 + q1;
                 }
+        R* yc = y + c * nnode + n0;
 #pragma unroll
-        for (int a = 0; a < NS; a++) {
-            const int32_t n = local_node<DIM>(n0, nn0, nn01, a);
-            if (!((bcmask[n] >> c) & 1)) atomicAdd(&y[(int64_t)c * nnode + n], Q[a]);
-        }
+        for (int a = 0; a < NS; a++)
+            if (!((fixed >> (4 * a + c)) & 1)) atomicAdd(yc + off[a], Q[a]);
     }
     return energy;
+}
+
+// Element tiles of one 256-thread block: 32 × 4 × 2 elements in 3D, 32 × 8 in 2D, x fastest
+// (a warp is one row of 32 elements: coalesced moment loads, no index divisions).
+template <int DIM>
+struct ApplyTile;
+template <>
+struct ApplyTile<3> {
+    static constexpr int X = 32, Y = 4, Z = 2;
+};
+template <>
+struct ApplyTile<2> {
+    static constexpr int X = 32, Y = 8, Z = 1;
+};
+
+// y += K x over the element tiles tile0, tile0 + tstride, … (blockDim.x must be 256).
+// Returns this thread's Σ x_eᵀ K_e x_e when kEnergy.
+template <int DIM, typename R, int kLoad = 0, bool kEnergy = true>
+__device__ __forceinline__ double apply_tiles(const MeshK& mk, const R* __restrict__ mom,
+                                              const uint8_t* __restrict__ bcmask, const R* __restrict__ x,
+                                              R* __restrict__ y, int64_t tile0, int64_t tstride) {
+    constexpr int TX = ApplyTile<DIM>::X, TY = ApplyTile<DIM>::Y, TZ = ApplyTile<DIM>::Z;
+    const int ntx = (mk.n[0] + TX - 1) / TX, nty = (mk.n[1] + TY - 1) / TY;
+    const int ntz = DIM == 3 ? (mk.n[2] + TZ - 1) / TZ : 1;
+    const int32_t ntiles = ntx * nty * ntz;
+    const int tx = threadIdx.x % TX, ty = (threadIdx.x / TX) % TY, tz = threadIdx.x / (TX * TY);
+    double en = 0.0;
+    for (int32_t tile = (int32_t)tile0; tile < ntiles; tile += (int32_t)tstride) {
+        const int rr = tile / ntx;
+        const int i = (tile - rr * ntx) * TX + tx, j = (rr % nty) * TY + ty, k = (rr / nty) * TZ + tz;
+        if (i < mk.n[0] && j < mk.n[1] && (DIM == 2 || k < mk.n[2]))
+            en += element_apply_scatter<DIM, R, kLoad, kEnergy>(mk, mom, bcmask, x, y, i, j, k,
+                                                                i + mk.n[0] * (j + mk.n[1] * k));
+    }
+    return en;
 }
 
 }  // namespace gg

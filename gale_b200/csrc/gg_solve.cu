@@ -163,12 +163,7 @@ k_cg_apply(MeshK mk, const V* __restrict__ mom, const uint8_t* __restrict__ bcma
            const V* __restrict__ p, V* __restrict__ Ap, KrylovScalars* s, double* part,
            unsigned int* counter) {
     if (s->done) return;
-    const int64_t nel = mk.nel;
-    double en = 0.0;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
-         e += (int64_t)gridDim.x * blockDim.x)
-        en += element_apply_scatter<DIM, V>(mk, mom, bcmask, p, Ap, e);
-    double acc[1] = {en};
+    double acc[1] = {apply_tiles<DIM, V>(mk, mom, bcmask, p, Ap, blockIdx.x, gridDim.x)};
     grid_reduce<1>(acc, part, counter, [=](double* t) {
         s->pAp = t[0];
         s->alpha = s->rz / t[0];
@@ -626,8 +621,12 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
                              [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
             }
         } else if (use_mg) {
-            rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it,
-                         [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+            rc = fused_fcg_enabled() ? run_fcg_fused(H, H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it)
+                                     : 1;
+            if (rc == 1)  // hierarchy outside the persistent kernel's limits
+                rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it,
+                             [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+            if (rc == GG_ERR_CUDA) return rc;
         } else {
             rc = run_cg<float>(H, "cg32", H.mk, H.mom32.as<float>(), H.kdiag32.as<float>(), H.r32.as<float>(),
                                H.e32.as<float>(), H.cgr32.as<float>(), H.z32.as<float>(), H.p32.as<float>(),

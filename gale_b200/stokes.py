@@ -350,7 +350,7 @@ class StokesProblem:
         y = np.zeros_like(t)
         g = np.zeros_like(w)
         loss = C.c_double(0)
-        nodes = C.c_int32(0)
+        nodes = C.c_int32(x.shape[2])  # checked against the level before the buffers are used
         self._check(self.lib.gg_learned_eval(self.h, level, x.shape[0], ptr(x, C.c_float), ptr(t, C.c_float),
                                              ptr(w, C.c_float), ptr(y, C.c_float), ptr(g, C.c_float),
                                              C.byref(loss), C.byref(nodes)))

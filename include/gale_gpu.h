@@ -328,7 +328,10 @@ GG_API int  gg_learned_weights(gg_handle* h, float* weights, int32_t* n);
 GG_API int  gg_learned_set_weights(gg_handle* h, int32_t level, const float* weights, int32_t n);
 /* Forward and backward of a batch on the network's grid (gradient check): inputs
  * [batch][1+dim][nodes], targets [batch][dim][nodes]; writes outputs, the gradient of
- * the normalised loss w.r.t. all parameters, the loss and the grid's node count.     */
+ * the normalised loss w.r.t. all parameters and the loss.  level must exist in the
+ * multigrid hierarchy (≤ 0: the default level).  *grid_nodes is in/out: on entry the
+ * node count the caller's buffers hold (checked against the level before any buffer is
+ * read; GG_ERR_INVALID on a mismatch), on return the level's node count.              */
 GG_API int  gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const float* inputs,
                             const float* targets, const float* weights, float* outputs,
                             float* gradient, double* loss, int32_t* grid_nodes);

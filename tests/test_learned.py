@@ -31,7 +31,7 @@ def level_grid(mesh, level):
 
 
 @pytest.mark.parametrize("make,level", [(lambda: workloads.creep_3d(n=16), 2),
-                                        (lambda: workloads.sinker_2d(n=32), 2)], ids=["3d", "2d"])
+                                        (lambda: workloads.sinker_2d(n=64), 2)], ids=["3d", "2d"])
 def test_gradients_match_cpu_reference(make, level):
     from oracle import learned_ref
     w = make()
