@@ -49,8 +49,8 @@ __device__ __forceinline__ int32_t local_node(int32_t n0, int32_t nn0, int32_t n
 // the modal coefficients and one component's Q.
 // The kernel is bound by instruction issue, not by bytes (the moments and vectors of a
 // 64³ level sit in L2), so the element index arrives as (i, j, k) without divisions,
-// node addresses are corner offsets from one base, and the BC bits of the 2^dim nodes
-// are read once.
+// node addresses are row bases plus the next word, the BC bits of the 2^dim nodes are
+// read once, and the monomials shared by ∂x_c/∂x_d and ∂x_d/∂x_c take one product.
 // kLoad selects how x is read: 0 plain (may use the read-only path), 1 through L2 only
 // (ld.global.cg), 2 cached weak loads (ld.global.ca).  A persistent kernel that wrote x in
 // an earlier phase of the same launch must not use 0: the non-coherent path is only valid
@@ -65,21 +65,27 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
     const int64_t nnode = mk.nnode, nel = mk.nel;
     const int32_t nn0 = mk.nn[0], nn01 = mk.nn[0] * mk.nn[1];
     const int32_t n0 = i + nn0 * j + (DIM == 3 ? nn01 * k : 0);
-    int32_t off[NS];
+    // corner a = (dx, dy, dz) bits; the NS/2 rows (dy, dz) start at n0 + rowoff, the x+1
+    // corner is the next word of the row
+    constexpr int NR = NS / 2;
+    int32_t rowoff[NR];
 #pragma unroll
-    for (int a = 0; a < NS; a++) off[a] = (a & 1) + ((a >> 1) & 1) * nn0 + (DIM == 3 ? ((a >> 2) & 1) * nn01 : 0);
+    for (int q = 0; q < NR; q++) rowoff[q] = (q & 1) * nn0 + (DIM == 3 ? ((q >> 1) & 1) * nn01 : 0);
     uint32_t fixed = 0;  // bit 4a + c: component c of corner a has a Dirichlet condition
 #pragma unroll
-    for (int a = 0; a < NS; a++) fixed |= (uint32_t)bcmask[n0 + off[a]] << (4 * a);
+    for (int q = 0; q < NR; q++) {
+        const uint8_t* br = bcmask + n0 + rowoff[q];
+        fixed |= ((uint32_t)br[0] | ((uint32_t)br[1] << 4)) << (8 * q);
+    }
 
     R m[DIM][NS];
 #pragma unroll
     for (int c = 0; c < DIM; c++) {
-        const R* xc = x + c * nnode + n0;
 #pragma unroll
-        for (int a = 0; a < NS; a++) {
-            const R* px = xc + off[a];
-            m[c][a] = kLoad == 1 ? __ldcg(px) : kLoad == 2 ? __ldca(px) : *px;
+        for (int q = 0; q < NR; q++) {
+            const R* xr = x + c * nnode + n0 + rowoff[q];
+            m[c][2 * q] = kLoad == 1 ? __ldcg(xr) : kLoad == 2 ? __ldca(xr) : xr[0];
+            m[c][2 * q + 1] = kLoad == 1 ? __ldcg(xr + 1) : kLoad == 2 ? __ldca(xr + 1) : xr[1];
         }
     }
     R M[NM];
@@ -127,11 +133,16 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
                     const int e0 = ((U >> 0) & 1) + ((T >> 0) & 1);
                     const int e1 = ((U >> 1) & 1) + ((T >> 1) & 1);
                     const int e2 = DIM == 3 ? ((U >> 2) & 1) + ((T >> 2) & 1) : 0;
+                    const bool td = !((T >> d) & 1), tc = !((T >> c) & 1);
                     if (c == d) {
-                        if (!((T >> c) & 1)) acc += g[c][c][T] * M[mom_slot<DIM>(e0, e1, e2)];
-                    } else {
-                        if (!((T >> d) & 1)) acc += g[c][d][T] * M[mom_slot<DIM>(e0, e1, e2)];
-                        if (!((T >> c) & 1)) acc += g[d][c][T] * M[mom_slot<DIM>(e0, e1, e2)];
+                        if (tc) acc += g[c][c][T] * M[mom_slot<DIM>(e0, e1, e2)];
+                    } else if (td && tc) {
+                        // monomials of both ∂x_c/∂x_d and ∂x_d/∂x_c: one product
+                        acc += (g[c][d][T] + g[d][c][T]) * M[mom_slot<DIM>(e0, e1, e2)];
+                    } else if (td) {
+                        acc += g[c][d][T] * M[mom_slot<DIM>(e0, e1, e2)];
+                    } else if (tc) {
+                        acc += g[d][c][T] * M[mom_slot<DIM>(e0, e1, e2)];
                     }
                 }
                 // σ_cc carries the factor 2 of D0
@@ -150,10 +161,12 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
                     Q[a] = q0 - q1;
                     Q[a | (1 << d)] = q0 + q1;
                 }
-        R* yc = y + c * nnode + n0;
 #pragma unroll
-        for (int a = 0; a < NS; a++)
-            if (!((fixed >> (4 * a + c)) & 1)) atomicAdd(yc + off[a], Q[a]);
+        for (int q = 0; q < NR; q++) {
+            R* yr = y + c * nnode + n0 + rowoff[q];
+            if (!((fixed >> (8 * q + c)) & 1)) atomicAdd(yr, Q[2 * q]);
+            if (!((fixed >> (8 * q + 4 + c)) & 1)) atomicAdd(yr + 1, Q[2 * q + 1]);
+        }
     }
     return energy;
 }
