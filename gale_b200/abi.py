@@ -135,6 +135,27 @@ class LearnStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+WEIGHTS_CONSTANT, WEIGHTS_DVC = 0, 1
+
+
+class Weights(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("resolution", C.c_int32 * 3)]
+
+
+class PcdvcParams(C.Structure):
+    _fields_ = [("upper_t", C.c_double), ("lower_t", C.c_double), ("max_splits", C.c_int32),
+                ("max_deletions", C.c_int32), ("split_in_interface_cells", C.c_int32),
+                ("delete_in_interface_cells", C.c_int32), ("inflow", C.c_int32)]
+
+
+class PcdvcStats(C.Structure):
+    _fields_ = [("points_before", C.c_int64), ("points_after", C.c_int64), ("splits", C.c_int64),
+                ("deletions", C.c_int64), ("ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def ptr(a, ctype=C.c_double):
     """Pointer to a contiguous numpy array (None stays NULL)."""
     if a is None:
@@ -183,6 +204,11 @@ ABI_FUNCTIONS = {
                            C.POINTER(C.c_int64), C.c_void_p, C.POINTER(C.c_char_p)], C.c_int),
     "gg_solve_batch": ([C.c_int32, C.POINTER(_P), C.POINTER(UzawaParams), C.c_int32, C.POINTER(_PD),
                         C.POINTER(_PD), C.POINTER(UzawaStats), _PI32], C.c_int),
+    "gg_set_weights": ([_P, C.POINTER(Weights)], C.c_int),
+    "gg_population_control": ([_P, C.POINTER(PcdvcParams), C.POINTER(PcdvcStats)], C.c_int),
+    "gg_point_count": ([_P, C.POINTER(C.c_int64)], C.c_int),
+    "gg_get_points": ([_P, _PD, _PI32, _PD], C.c_int),
+    "gg_get_integration_points": ([_P, _PD, _PD], C.c_int),
     "gg_learned_train": ([_P, C.POINTER(LearnParams), C.POINTER(LearnStats)], C.c_int),
     "gg_learned_weights": ([_P, C.POINTER(C.c_float), _PI32], C.c_int),
     "gg_learned_set_weights": ([_P, C.c_int32, C.POINTER(C.c_float), C.c_int32], C.c_int),

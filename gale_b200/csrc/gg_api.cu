@@ -292,6 +292,7 @@ int gg_set_points(gg_handle* h, int64_t n, const double* coords, const int32_t* 
         GG_CUDA(cudaStreamSynchronize(H.stream));
         H.located = false;
         H.built = false;
+        H.dvc_valid = false;
     })
     return GG_OK;
 }
@@ -330,18 +331,21 @@ int gg_locate(gg_handle* h, uint32_t* owning_cell) {
     Handle& H = h->H;
     if (H.np == 0) return gg::set_error(H, GG_ERR_STATE, "points not set");
     int64_t outside = 0;
+    int rc = GG_OK;
     GG_TRY(h, {
         outside = gg::locate_and_sort(H);
         H.np_in = H.np - outside;
+        H.dvc_valid = false;
+        if (!outside && H.weights.mode == GG_WEIGHTS_DVC) rc = gg::dvc_update(H, nullptr, nullptr);
         if (owning_cell) {
             GG_CUDA(cudaMemcpyAsync(owning_cell, H.cell.p, sizeof(uint32_t) * H.np, cudaMemcpyDeviceToHost, H.stream));
             GG_CUDA(cudaStreamSynchronize(H.stream));
         }
     })
-    H.located = outside == 0;
+    H.located = outside == 0 && rc == GG_OK;
     H.built = false;
     if (outside) return gg::set_error(H, GG_ERR_OUT_OF_DOMAIN, std::to_string(outside) + " material points outside the mesh");
-    return GG_OK;
+    return rc;
 }
 
 }  // extern "C"

@@ -371,6 +371,110 @@ int gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const float* inp
     return rc;
 }
 
+int gg_set_weights(gg_handle* h, const gg_weights* w) {
+    if (!h || !w) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (w->mode != GG_WEIGHTS_CONSTANT && w->mode != GG_WEIGHTS_DVC)
+        return gg::err(H, GG_ERR_INVALID, "weights mode");
+    if (w->mode == GG_WEIGHTS_DVC) {
+        const int nz = H.dim == 3 ? w->resolution[2] : 1;
+        if (w->resolution[0] < 1 || w->resolution[1] < 1 || nz < 1 || w->resolution[0] > 64 || w->resolution[1] > 64 ||
+            nz > 64 || w->resolution[0] * w->resolution[1] * nz > 1024)
+            return gg::err(H, GG_ERR_INVALID, "DVC resolution: at most 64 per axis and 1024 cells per element");
+    }
+    H.weights = *w;
+    // the integration points change: locate again before the next build
+    H.located = false;
+    H.built = false;
+    H.dvc_valid = false;
+    return GG_OK;
+}
+
+int gg_population_control(gg_handle* h, const gg_pcdvc_params* prm, gg_pcdvc_stats* stats) {
+    if (!h || !prm) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (H.weights.mode != GG_WEIGHTS_DVC) return gg::err(H, GG_ERR_STATE, "population control needs GG_WEIGHTS_DVC");
+    if (!H.located) return gg::err(H, GG_ERR_STATE, "gg_locate has not succeeded");
+    int rc = GG_OK;
+    gg_pcdvc_stats st{};
+    GG_TRY2(h, {
+        GG_CUDA(cudaEventRecord(H.ev0, H.stream));
+        rc = gg::dvc_update(H, prm, &st);
+        GG_CUDA(cudaEventRecord(H.ev1, H.stream));
+        GG_CUDA(cudaEventSynchronize(H.ev1));
+        float ms = 0.f;
+        GG_CUDA(cudaEventElapsedTime(&ms, H.ev0, H.ev1));
+        st.ms = ms;
+    })
+    H.built = false;
+    if (rc != GG_OK) H.located = false;
+    if (stats) *stats = st;
+    return rc;
+}
+
+int gg_point_count(gg_handle* h, int64_t* n) {
+    if (!h || !n) return GG_ERR_INVALID;
+    *n = h->H.np;
+    return GG_OK;
+}
+
+int gg_get_points(gg_handle* h, double* coords, int32_t* material, double* plastic_strain) {
+    if (!h) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (H.np == 0) return gg::err(H, GG_ERR_STATE, "points not set");
+    GG_TRY2(h, {
+        if (coords)
+            GG_CUDA(cudaMemcpyAsync(coords, H.coords.p, sizeof(double) * H.np * H.dim, cudaMemcpyDeviceToHost, H.stream));
+        if (material)
+            GG_CUDA(cudaMemcpyAsync(material, H.mat_in.p, sizeof(int32_t) * H.np, cudaMemcpyDeviceToHost, H.stream));
+        if (plastic_strain)
+            GG_CUDA(cudaMemcpyAsync(plastic_strain, H.ps_in.p, sizeof(double) * H.np, cudaMemcpyDeviceToHost, H.stream));
+        GG_CUDA(cudaStreamSynchronize(H.stream));
+    })
+    return GG_OK;
+}
+
+}  // extern "C"
+
+namespace gg {
+namespace {
+// sorted integration points → point order; constant weights from the element counts
+__global__ void k_int_points(int64_t np, int dim, const int32_t* __restrict__ perm, const int32_t* __restrict__ cell_s,
+                             const int32_t* __restrict__ offsets, const double* __restrict__ xi_s,
+                             const double* __restrict__ w_s, double* __restrict__ xi, double* __restrict__ w) {
+    const double wscale = (double)(1 << dim);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t p = perm[i];
+        for (int d = 0; d < dim; d++) xi[(int64_t)p * dim + d] = xi_s[(int64_t)d * np + i];
+        const int32_t e = cell_s[i];
+        w[p] = w_s ? w_s[i] : wscale / (double)(offsets[e + 1] - offsets[e]);
+    }
+}
+}  // namespace
+}  // namespace gg
+
+extern "C" {
+
+int gg_get_integration_points(gg_handle* h, double* xi, double* weight) {
+    if (!h || !xi || !weight) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (!H.located) return gg::err(H, GG_ERR_STATE, "gg_locate has not succeeded");
+    GG_TRY2(h, {
+        DBuf dx, dw;
+        dx.ensure(sizeof(double) * H.np * H.dim);
+        dw.ensure(sizeof(double) * H.np);
+        gg::k_int_points<<<gg::grid_for(H.np, 256), 256, 0, H.stream>>>(
+            H.np, H.dim, H.perm.as<int32_t>(), H.cell_s.as<int32_t>(), H.offsets.as<int32_t>(), H.xi_s.as<double>(),
+            H.weights.mode == GG_WEIGHTS_DVC && H.dvc_valid ? H.w_s.as<double>() : nullptr, dx.as<double>(),
+            dw.as<double>());
+        GG_CUDA(cudaGetLastError());
+        GG_CUDA(cudaMemcpyAsync(xi, dx.p, sizeof(double) * H.np * H.dim, cudaMemcpyDeviceToHost, H.stream));
+        GG_CUDA(cudaMemcpyAsync(weight, dw.p, sizeof(double) * H.np, cudaMemcpyDeviceToHost, H.stream));
+        GG_CUDA(cudaStreamSynchronize(H.stream));
+    })
+    return GG_OK;
+}
+
 int gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_launch) {
     if (!h || !ms_per_launch || reps < 1) return GG_ERR_INVALID;
     Handle& H = h->H;

@@ -215,7 +215,7 @@ k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
                 R* __restrict__ mom, R* __restrict__ kdiag, double* __restrict__ sdiag,
                 double* __restrict__ f, double* __restrict__ eta_s, double* __restrict__ incr_s,
                 uint8_t* __restrict__ yld_s, int32_t* __restrict__ flag,
-                const gg_material* __restrict__ materials) {
+                const gg_material* __restrict__ materials, const double* __restrict__ w_s) {
     constexpr int NM = n_moments<DIM>();
     constexpr int NEN = 1 << DIM;
     __shared__ R s_c[kChunk];
@@ -259,7 +259,8 @@ k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
             const gg_material& m = materials[mi];
             PointOut po = run_rheologies<DIM, R>(mk, m, ijk, pe, xi, T, pu, pp, ps_s[i], prev);
             const int32_t cnt = offsets[pe + 1] - offsets[pe];
-            const double w = wscale / (double)cnt;  // _ConstantWeights_Calculate
+            // per-point weight (DVCWeights) or _ConstantWeights_Calculate
+            const double w = w_s ? w_s[i] : wscale / (double)cnt;
             s_c[i - cs] = (R)(w * mk.detJ) * (R)po.eta;
 #pragma unroll
             for (int d = 0; d < DIM; d++) s_xi[d][i - cs] = xi[d];
@@ -398,7 +399,8 @@ static void launch_build(Handle& H, int prev, const double* pu, const double* pp
         H.mk, nel, H.offsets.as<int32_t>(), H.xi_s.as<double>(), H.np_in, H.mat_s.as<int32_t>(),
         H.ps_s.as<double>(), T, pu, pp, prev, H.force.gravity, g[0], g[1], g[2], H.force.rayleigh,
         f ? 1 : 0, mom, kdiag, sdiag, f, outputs ? H.eta_s.as<double>() : nullptr,
-        H.incr_s.as<double>(), H.yld_s.as<uint8_t>(), H.flag.as<int32_t>(), H.d_materials.as<gg_material>());
+        H.incr_s.as<double>(), H.yld_s.as<uint8_t>(), H.flag.as<int32_t>(), H.d_materials.as<gg_material>(),
+        H.weights.mode == GG_WEIGHTS_DVC && H.dvc_valid ? H.w_s.as<double>() : nullptr);
     GG_CUDA(cudaGetLastError());
 }
 

@@ -81,6 +81,12 @@ struct Handle {
     DBuf coords, mat_in, ps_in, cell, perm, cell_s, xi_s, mat_s, ps_s, eta_s, incr_s, yld_s;
     DBuf offsets, fill, scan_tmp, flag;
     bool located = false;
+    // integration weights (gg_dvc.cu): with GG_WEIGHTS_DVC, xi_s holds the Voronoi
+    // centroids and w_s the volumes of the sorted points once dvc_valid; xi_pts keeps
+    // the material points' own ξ, from which the diagrams grow
+    gg_weights weights{GG_WEIGHTS_CONSTANT, {10, 10, 10}};
+    bool dvc_valid = false;
+    DBuf w_s, xi_pts, dvc_cent, dvc_keep, dvc_err, dvc_nsplit, dvc_ndel, dvc_parent, dvc_new, dvc_scan, dvc_scan2;
 
     // operator
     DBuf mom64, mom32, kdiag64, kdiag32, sdiag, hvec, f;

@@ -37,6 +37,11 @@ __device__ __forceinline__ int64_t elem_node(const MeshK& mk, const int* ijk, in
 
 // ---- host drivers ------------------------------------------------------------------
 int64_t locate_and_sort(Handle& H);
+// out = exclusive prefix sum of in[0..n) on the device; *total_host = the sum.
+void exclusive_scan_i32(Handle& H, const int32_t* in, int32_t* out, int64_t n, DBuf& tmp, int32_t* total_host);
+// DVCWeights of the located points (prm = nullptr) or PCDVC population control with the
+// rebuilt and re-located point set (gg_dvc.cu).  GG_OK or a status (message set).
+int dvc_update(Handle& H, const gg_pcdvc_params* prm, gg_pcdvc_stats* stats);
 
 // Per-point rheology + moments + force + diagonals.  precision GG_PRECISION_FP64 fills
 // mom64/kdiag64/sdiag/f/eta; GG_PRECISION_MIXED additionally fills mom32/kdiag32 with

@@ -199,6 +199,23 @@ int grid_for(int64_t n, int block) {
     return (int)g;
 }
 
+// out = exclusive prefix sum of in[0..n) (device), *total_host = the sum (synchronises).
+void exclusive_scan_i32(Handle& H, const int32_t* in, int32_t* out, int64_t n, DBuf& tmp, int32_t* total_host) {
+    cudaStream_t st = H.stream;
+    const int64_t nblk = (n + 1023) / 1024;
+    tmp.ensure(sizeof(int32_t) * (nblk + 2));
+    if (n > 0) {
+        k_scan_blocks<<<(int)nblk, 1024, 0, st>>>(in, n, out, tmp.as<int32_t>());
+        k_scan_sums<<<1, 1024, 0, st>>>(tmp.as<int32_t>(), nblk, tmp.as<int32_t>() + nblk);
+        k_scan_add<<<(int)nblk, 1024, 0, st>>>(out, n, tmp.as<int32_t>(), tmp.as<int32_t>() + nblk);
+        GG_CUDA(cudaGetLastError());
+        GG_CUDA(cudaMemcpyAsync(total_host, tmp.as<int32_t>() + nblk, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    } else {
+        *total_host = 0;
+    }
+    GG_CUDA(cudaStreamSynchronize(st));
+}
+
 // Locate + stable counting sort + gather.  Returns number of points outside the mesh.
 int64_t locate_and_sort(Handle& H) {
     const int64_t np = H.np, nel = H.nel;

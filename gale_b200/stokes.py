@@ -260,6 +260,48 @@ class StokesProblem:
     def set_body_force(self, bf):
         self._check(self.lib.gg_set_body_force(self.h, C.byref(bf)))
 
+    # integration weights and population control (DVCWeights / PCDVC)
+    def set_weights(self, mode="constant", resolution=10):
+        """mode "constant" (ConstantWeights) or "dvc" (DVCWeights with `resolution` cells
+        per element axis, an int or a per-axis sequence); call locate() afterwards."""
+        w = abi.Weights()
+        w.mode = {"constant": abi.WEIGHTS_CONSTANT, "dvc": abi.WEIGHTS_DVC}[mode]
+        res = [resolution] * 3 if np.isscalar(resolution) else list(resolution) + [1] * (3 - len(resolution))
+        for d in range(3):
+            w.resolution[d] = int(res[d])
+        self._check(self.lib.gg_set_weights(self.h, C.byref(w)))
+
+    def population_control(self, upperT=25.0, lowerT=0.6, maxSplits=3, maxDeletions=2,
+                           splitInInterfaceCells=False, deleteInInterfaceCells=False, Inflow=False):
+        """PCDVC with the reference's XML parameter names (PCDVC.cxx:233-276 defaults)."""
+        p = abi.PcdvcParams()
+        p.upper_t, p.lower_t = upperT, lowerT
+        p.max_splits, p.max_deletions = maxSplits, maxDeletions
+        p.split_in_interface_cells = int(splitInInterfaceCells)
+        p.delete_in_interface_cells = int(deleteInInterfaceCells)
+        p.inflow = int(Inflow)
+        st = abi.PcdvcStats()
+        self._check(self.lib.gg_population_control(self.h, C.byref(p), C.byref(st)))
+        self.np = st.points_after
+        return st.as_dict()
+
+    def points(self):
+        n = C.c_int64(0)
+        self._check(self.lib.gg_point_count(self.h, C.byref(n)))
+        x = np.zeros((n.value, self.dim))
+        m = np.zeros(n.value, dtype=np.int32)
+        ps = np.zeros(n.value)
+        self._check(self.lib.gg_get_points(self.h, ptr(x), ptr(m, C.c_int32), ptr(ps)))
+        return x, m, ps
+
+    def integration_points(self):
+        n = C.c_int64(0)
+        self._check(self.lib.gg_point_count(self.h, C.byref(n)))
+        xi = np.zeros((n.value, self.dim))
+        w = np.zeros(n.value)
+        self._check(self.lib.gg_get_integration_points(self.h, ptr(xi), ptr(w)))
+        return xi, w
+
     # pipeline
     def locate(self) -> np.ndarray:
         cell = np.empty(self.np, dtype=np.uint32)

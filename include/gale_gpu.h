@@ -255,6 +255,53 @@ GG_API int  gg_locate_noalloc(const gg_mesh_desc* mesh, int64_t n_points, const 
                               uint32_t* d_cell, int32_t* d_offsets, int32_t* d_order,
                               int64_t* n_outside, void* stream, const char** message);
 
+/* ---- integration weights and population control (A13) ------------------------------
+ * GG_WEIGHTS_CONSTANT: the material points are the integration points with
+ * w = 2^dim / points-in-element (_ConstantWeights_Calculate, PICellerator/Weights/src/
+ * ConstantWeights.cxx:178-187); the default.
+ * GG_WEIGHTS_DVC: DVCWeights (PICellerator/Weights/src/DVCWeights.cxx:788-953): each
+ * element's [-1,1]^dim is cut into resolution[0]×resolution[1](×resolution[2]) cells, a
+ * discrete Voronoi diagram is grown from the element's points, and every integration
+ * point moves to the centroid of its region with the region's volume as weight.  gg_locate
+ * recomputes them, and every operator build uses them.  Limits: ≤ 1024 grid cells and
+ * ≤ 254 points per element (GG_ERR_INVALID otherwise).                                 */
+enum { GG_WEIGHTS_CONSTANT = 0, GG_WEIGHTS_DVC = 1 };
+typedef struct {
+    int32_t mode;
+    int32_t resolution[3];   /* DVCWeights resolutionX/Y/Z (reference default 10)          */
+} gg_weights;
+GG_API int  gg_set_weights(gg_handle* h, const gg_weights* weights);
+
+/* PCDVC population control (PICellerator/Utils/src/PCDVC.cxx:656-1512), run after
+ * gg_locate in GG_WEIGHTS_DVC mode: per element, points whose Voronoi volume is above
+ * upper_t % of the element are split (the new point, a copy of its parent, sits at the
+ * parent region's centroid; at most max_splits per element) and points below lower_t %
+ * are deleted (at most max_deletions, decreasing point index first); elements whose
+ * points carry more than one material split/delete only when the *_in_interface_cells
+ * flags allow it.  Changed elements get a new diagram.  The point set is then rebuilt:
+ * the points that survive in their previous order, followed by the new points (element
+ * order, then their parents' order), and re-located; gg_point_count / gg_get_points read
+ * it back.  The Inflow branch (random re-seeding) is not provided: inflow != 0 returns
+ * GG_ERR_INVALID.                                                                         */
+typedef struct {
+    double  upper_t, lower_t;          /* upperT (25), lowerT (0.6): % of the element volume */
+    int32_t max_splits, max_deletions; /* maxSplits (3), maxDeletions (2)                   */
+    int32_t split_in_interface_cells;  /* splitInInterfaceCells (0)                         */
+    int32_t delete_in_interface_cells; /* deleteInInterfaceCells (0)                        */
+    int32_t inflow;                    /* Inflow: must be 0                                 */
+} gg_pcdvc_params;
+typedef struct {
+    int64_t points_before, points_after, splits, deletions;
+    double  ms;                        /* device time of the whole call                     */
+} gg_pcdvc_stats;
+GG_API int  gg_population_control(gg_handle* h, const gg_pcdvc_params* params, gg_pcdvc_stats* stats);
+GG_API int  gg_point_count(gg_handle* h, int64_t* n);
+/* The current points: coords [n*dim], material [n], plastic strain [n] (each nullable). */
+GG_API int  gg_get_points(gg_handle* h, double* coords, int32_t* material, double* plastic_strain);
+/* Integration point of every material point (point order): local coordinates xi [n*dim]
+ * and weight [n] as the operator build uses them.                                        */
+GG_API int  gg_get_integration_points(gg_handle* h, double* xi, double* weight);
+
 /* ---- operator build ---------------------------------------------------------------
  * Replaces the assembleStiffnessMatrix entry point (__StiffnessMatrix_NewAssemble,
  * StiffnessMatrix.cxx:2016-2200) for k_matrix, g_matrix and the Uzawa preconditioner,

@@ -180,6 +180,19 @@ static void local_to_global(const mesh_t* M, const int* ijk, const double* xi, d
     }
 }
 
+/* Global coordinates of local points xi [n][dim] in elements cell [n].               */
+void or_local_to_global(const gg_mesh_desc* md, int64_t n, const uint32_t* cell, const double* xi, double* x) {
+    mesh_t M;
+    mesh_init(&M, md);
+    for (int64_t p = 0; p < n; p++) {
+        int ijk[3];
+        elem_ijk(&M, cell[p], ijk);
+        double g[3];
+        local_to_global(&M, ijk, xi + p * M.dim, g);
+        for (int d = 0; d < M.dim; d++) x[p * M.dim + d] = g[d];
+    }
+}
+
 /* -------------------------------------------------------------- A1 locate --- */
 /* Num_Approx (StGermain/Base/Foundation/src/Numerics.cxx:38-43), ε = 1e-12.         */
 static int num_approx(double var, double val) {

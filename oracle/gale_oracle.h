@@ -69,6 +69,8 @@ int  or_picard(or_problem* P, const gg_picard_params* pic, const gg_uzawa_params
 int  or_inner_solve(or_problem* P, const double* b, double* x, double rtol, int32_t maxit);
 int  or_advect(or_problem* P, double dt, int32_t order, const double* u, double* coords_out);
 int  or_courant_dt(or_problem* P, const double* u, double* dt);
+/* FeMesh_CoordLocalToGlobal of points xi [n][dim] in elements cell [n].            */
+void or_local_to_global(const gg_mesh_desc* m, int64_t n, const uint32_t* cell, const double* xi, double* x);
 const char* or_last_error(void);
 
 #ifdef __cplusplus

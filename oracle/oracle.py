@@ -57,7 +57,21 @@ _SIG = {
     "or_advect": ([_P, C.c_double, C.c_int32, _PD, _PD], C.c_int),
     "or_courant_dt": ([_P, _PD, _PD], C.c_int),
     "or_last_error": ([], C.c_char_p),
+    "or_local_to_global": ([C.POINTER(abi.MeshDesc), C.c_int64, _PU32, _PD, _PD], None),
+    "od_dvc_cell": ([C.c_int32, _PI32, C.c_int32, _PD, _PD, _PI32], C.c_int),
+    "od_dvc_cell_volume": ([C.c_int32, _PI32], C.c_double),
 }
+
+
+class PcdvcParams(C.Structure):
+    """od_pcdvc_params (oracle/dvc_oracle.h)."""
+    _fields_ = [("upper_t", C.c_double), ("lower_t", C.c_double), ("max_splits", C.c_int32),
+                ("max_deletions", C.c_int32), ("split_in_interface_cells", C.c_int32),
+                ("delete_in_interface_cells", C.c_int32)]
+
+
+_SIG["od_pcdvc_cell"] = ([C.c_int32, _PI32, C.POINTER(PcdvcParams), C.c_int32, _PD, _PI32, _PI64, _PI32, _PD, _PD,
+                          _PD, _PI32, _PI32, _PI32], C.c_int)
 
 
 def build():
@@ -259,3 +273,116 @@ class OracleProblem:
         dt = C.c_double(0)
         _check(lib().or_courant_dt(self.h, ptr(u), C.byref(dt)))
         return dt.value
+
+
+# ---- A13: discrete-Voronoi weights and population control --------------------------
+def dvc_cell(dim, res, xi):
+    """Voronoi centroids [n][dim] and weights [n] of one element's points xi [n][dim]."""
+    xi = f64(xi).reshape(-1, dim)
+    n = xi.shape[0]
+    r = np.ascontiguousarray(list(res) + [1] * (3 - len(res)), dtype=np.int32)
+    cent = np.zeros((n, dim))
+    cnt = np.zeros(n, dtype=np.int32)
+    rc = lib().od_dvc_cell(dim, ptr(r, C.c_int32), n, ptr(xi), ptr(cent), ptr(cnt, C.c_int32))
+    if rc:
+        raise OracleError(rc, "od_dvc_cell")
+    return cent, cnt * lib().od_dvc_cell_volume(dim, ptr(r, C.c_int32))
+
+
+def _cells_of(mesh, coords):
+    cell = locate(mesh, coords)
+    nel = int(np.prod([mesh.elements[d] for d in range(mesh.dim)]))
+    offs = np.zeros(nel + 1, dtype=np.int64)
+    order = np.zeros(len(cell), dtype=np.int64)
+    lib().or_cell_lists(len(cell), ptr(cell, C.c_uint32), nel, ptr(offs, C.c_int64), ptr(order, C.c_int64))
+    xi = np.zeros((len(cell), mesh.dim))
+    lib().or_local_coords(C.byref(mesh), len(cell), ptr(f64(coords)), ptr(cell, C.c_uint32), ptr(xi))
+    return cell, offs, order, xi
+
+
+def dvc_weights(mesh, coords, res):
+    """DVCWeights on every element: per point (input order) the integration position (the
+    centroid of its Voronoi region) and weight (its volume)."""
+    dim = mesh.dim
+    cell, offs, order, xi = _cells_of(mesh, coords)
+    cent = np.zeros((len(cell), dim))
+    w = np.zeros(len(cell))
+    for e in range(len(offs) - 1):
+        idx = order[offs[e]:offs[e + 1]]
+        if len(idx):
+            c, ww = dvc_cell(dim, res, xi[idx])
+            cent[idx], w[idx] = c, ww
+    return cent, w
+
+
+def population_control(mesh, coords, material, plastic_strain, params, res):
+    """PCDVC (Inflow off) over all elements in element order, then the new point set:
+    points that survive in input order, followed by the new points (element order, then
+    their parents' order in the element list), each with its integration position and
+    weight from its element's final Voronoi diagram.  Returns a dict."""
+    dim = mesh.dim
+    coords = f64(coords).reshape(-1, dim)
+    material = np.ascontiguousarray(material, dtype=np.int32)
+    ps = np.zeros(len(coords)) if plastic_strain is None else f64(plastic_strain)
+    cell, offs, order, xi = _cells_of(mesh, coords)
+    r = np.ascontiguousarray(list(res) + [1] * (3 - len(res)), dtype=np.int32)
+    keep = np.zeros(len(coords), dtype=bool)
+    cent = np.zeros((len(coords), dim))
+    w = np.zeros(len(coords))
+    new_parent, new_cell, new_xi, new_cent, new_w = [], [], [], [], []
+    nsplit = ndel = 0
+    prm = params
+    for e in range(len(offs) - 1):
+        idx = order[offs[e]:offs[e + 1]]
+        n = len(idx)
+        if n == 0:
+            continue
+        cap = n + prm.max_splits + 1
+        src = np.zeros(cap, dtype=np.int32)
+        oxi = np.zeros((cap, dim))
+        oc = np.zeros((cap, dim))
+        ow = np.zeros(cap)
+        no, ns, nd = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        exi = np.ascontiguousarray(xi[idx])
+        emat = np.ascontiguousarray(material[idx])
+        eidx = np.ascontiguousarray(idx, dtype=np.int64)
+        rc = lib().od_pcdvc_cell(dim, ptr(r, C.c_int32), C.byref(prm), n, ptr(exi), ptr(emat, C.c_int32),
+                                 ptr(eidx, C.c_int64), ptr(src, C.c_int32), ptr(oxi), ptr(oc), ptr(ow),
+                                 C.byref(no), C.byref(ns), C.byref(nd))
+        if rc:
+            raise OracleError(rc, f"od_pcdvc_cell (element {e})")
+        nsplit += ns.value
+        ndel += nd.value
+        news = []
+        for k in range(no.value):
+            if src[k] >= 0:
+                p = idx[src[k]]
+                keep[p] = True
+                cent[p], w[p] = oc[k], ow[k]
+            else:
+                news.append((-1 - src[k], k))
+        for slot, k in sorted(news):
+            new_parent.append(idx[slot])
+            new_cell.append(e)
+            new_xi.append(oxi[k])
+            new_cent.append(oc[k])
+            new_w.append(ow[k])
+    surv = np.nonzero(keep)[0]
+    m = len(new_parent)
+    if m:
+        nxi = np.ascontiguousarray(np.array(new_xi).reshape(m, dim))
+        ncell = np.ascontiguousarray(new_cell, dtype=np.uint32)
+        ncoords = np.zeros((m, dim))
+        lib().or_local_to_global(C.byref(mesh), m, ptr(ncell, C.c_uint32), ptr(nxi), ptr(ncoords))
+        par = np.array(new_parent, dtype=np.int64)
+    else:
+        ncoords = np.zeros((0, dim))
+        par = np.zeros(0, dtype=np.int64)
+    return {
+        "coords": np.concatenate([coords[surv], ncoords]),
+        "material": np.concatenate([material[surv], material[par]]).astype(np.int32),
+        "plastic_strain": np.concatenate([ps[surv], ps[par]]),
+        "xi": np.concatenate([cent[surv], np.array(new_cent).reshape(m, dim)]),
+        "weight": np.concatenate([w[surv], np.array(new_w)]),
+        "splits": nsplit, "deletions": ndel,
+    }
