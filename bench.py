@@ -234,7 +234,18 @@ def gale_arm(args):
     t_b64 = dev_time(lambda: G.build_operator("fp64"))
     G.solve(UzawaSolver(tolerance=1e-3, precision="fp64", inner="jacobi"))  # a stored velocity to advect with
     t_adv = dev_time(lambda: G._check(G.lib.gg_advect(G.h, 1e-6, 2, None, None)))
+    # A13 on the same points: DVCWeights (on top of the location) and one PCDVC pass
+    D = w.apply(StokesProblem(w.mesh))
+    D.set_weights("dvc", 10)
+    with _dev_timer() as td:
+        D.locate()
+    with _dev_timer() as tp:
+        pc = D.population_control()
+    D.close()
     components = {
+        "A13_dvc_weights": {"s": max(td.t - t_loc, 0.0), "elements_per_s": G.nel / max(td.t - t_loc, 1e-9),
+                            "what": "10^3-cell discrete Voronoi diagram per element (locate excluded)"},
+        "A13_population_control": {"s": tp.t, "splits": pc["splits"], "deletions": pc["deletions"]},
         "A1_A2_locate_sort": {"s": t_loc, "points_per_s": G.np / t_loc},
         "A3_A8_build_mixed": {"s": t_bm, "points_per_s": G.np / t_bm,
                               "what": "per-point rheology, FP64 + FP32 moments, diagonals, force"},
@@ -381,7 +392,9 @@ def main():
     ap.add_argument("--fp64", action="store_true", help="with --profile-solve --inner jacobi: plain FP64 path")
     ap.add_argument("--profile-apply", type=int, default=None, metavar="REPS",
                     help="build the operator and run REPS FP32 K applies back to back (ncu captures)")
-    ap.add_argument("--config", default="creep", choices=["creep", "batch"])
+    ap.add_argument("--config", default="creep", choices=["creep", "batch", "picard", "timestep"])
+    ap.add_argument("--max-outer", type=int, default=10000,
+                    help="--config timestep: Uzawa maxIterations for the 1e6-contrast solve")
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--serial-sample", type=int, default=24)
@@ -397,6 +410,10 @@ def main():
         profile_apply(args)
     elif args.config == "batch":
         batch_arm(args)
+    elif args.config == "picard":
+        picard_arm(args)
+    elif args.config == "timestep":
+        timestep_arm(args)
     else:
         gale_arm(args)
 
@@ -449,6 +466,108 @@ def batch_arm(args):
             "one_at_a_time_plain_fp64_s_per_problem": t_serial,
             "speedup_vs_one_at_a_time": t_serial * total / t_batch,
             "serial_sample": ns}), flush=True)
+
+
+def _dev_timer():
+    import torch
+
+    class T:
+        def __enter__(self):
+            torch.cuda.synchronize()
+            self.s, self.e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            self.s.record()
+            return self
+
+        def __exit__(self, *a):
+            self.e.record()
+            torch.cuda.synchronize()
+            self.t = self.s.elapsed_time(self.e) / 1e3
+
+    return T()
+
+
+def picard_arm(args):
+    """C3: 2D viscoplastic extension, 256×64 elements, 40 points per element, three layers
+    (Drucker–Prager upper crust with strain weakening), side walls pulled at ±1, 20 Picard
+    steps to rtol 1e-5 (Uzawa rtol 1e-5).  The fast path (FP32/FP64 refinement, multigrid,
+    the learned correction judged per solve) against the plain FP64 path; device-timed."""
+    from gale_b200 import workloads
+    from gale_b200.stokes import StokesProblem, UzawaSolver
+    w = workloads.extension_2d()
+    res = {}
+    sol = {}
+    for name, prm in (("fast", UzawaSolver(tolerance=1e-5, precision="mixed", inner=args.inner)),
+                      ("plain_fp64", UzawaSolver(tolerance=1e-5, precision="fp64", inner="jacobi"))):
+        G = w.apply(StokesProblem(w.mesh))
+        G.locate()
+        if name == "fast" and args.inner == "learned":
+            G.build_operator("mixed")
+            G.train_learned(level=2, n_rhs=4, iters_per_rhs=6, epochs=40)
+        with _dev_timer() as t:
+            u, p, st = G.picard(w.picard, prm)
+        inc, y = G.point_yield()
+        res[name] = {"s": t.t, "picard_iterations": st["iterations"], "picard_residual": st["residual"],
+                     "outer_iterations": st["outer_iterations"], "inner_iterations": st["inner_iterations"],
+                     "yielded_fraction": float(np.mean(y))}
+        sol[name] = u
+        G.close()
+    print(json.dumps({
+        "metric": "C3 Picard (20 steps) time: fast vs plain FP64, 1 B200", "value": res["fast"]["s"], "unit": "s",
+        "higher_is_better": False, "dtype": "f32/f64", "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": "extension_2d: 256x64 Q1-P0, 40 points/element, 3 layers, DP + strain weakening, "
+                               "walls +/-1, 20 Picard steps rtol 1e-5", "inner": args.inner},
+        "fast": res["fast"], "plain_fp64": res["plain_fp64"],
+        "speedup": res["plain_fp64"]["s"] / res["fast"]["s"],
+        "rel_l2_u_fast_vs_plain": float(np.linalg.norm(sol["fast"] - sol["plain_fp64"]) /
+                                        np.linalg.norm(sol["plain_fp64"]))}), flush=True)
+
+
+def timestep_arm(args):
+    """C5: one full time step of the 3D subduction-like model (128×64×128 elements on
+    [0,2]×[0,1]×[0,2], 27 points per element, slab η=1e4 with a weak η=1e-2 channel in an
+    η=1 mantle): locate + DVC weights, PCDVC population control, operator build, Uzawa to
+    rtol 1e-6 (FP32/FP64 refinement + multigrid; `--max-outer` Uzawa iterations), RK2
+    advection, re-location.  Each stage device-timed."""
+    from gale_b200 import workloads
+    from gale_b200.stokes import GaleError, StokesProblem, UzawaSolver
+    w = workloads.subduction_3d()
+    G = w.apply(StokesProblem(w.mesh))
+    G.set_weights("dvc", 10)
+    stages = {}
+    with _dev_timer() as t:
+        G.locate()
+    stages["locate_dvc_weights_s"] = t.t
+    with _dev_timer() as t:
+        pc = G.population_control()
+    stages["population_control_s"] = t.t
+    with _dev_timer() as t:
+        G.build_operator("mixed")
+    stages["build_s"] = t.t
+    prm = UzawaSolver(tolerance=1e-6, precision="mixed", inner="mg", maxIterations=args.max_outer)
+    converged = True
+    with _dev_timer() as t:
+        try:
+            u, p, st = G.solve(prm)
+        except GaleError as e:
+            converged, st = False, getattr(e, "stats", {})
+            u = None
+    stages["uzawa_s"] = t.t
+    if u is not None:
+        dt = G.courant_dt(u)
+        with _dev_timer() as t:
+            G._check(G.lib.gg_advect(G.h, dt, 2, None, None))
+        stages["advect_rk2_s"] = t.t
+        with _dev_timer() as t:
+            G.locate()
+        stages["relocate_dvc_s"] = t.t
+    print(json.dumps({
+        "metric": "C5 time step (3D subduction, 1e6 contrast): seconds, 1 B200", "value": sum(stages.values()),
+        "unit": "s", "higher_is_better": False, "dtype": "f32/f64", "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": "subduction_3d: 128x64x128 Q1-P0, 27 points/element, slab 1e4 + channel 1e-2",
+                   "points": int(G.np), "uzawa_rtol": 1e-6, "max_outer": args.max_outer},
+        "stages": stages, "population_control": pc, "converged": converged,
+        "uzawa": {k: st.get(k) for k in ("outer_iterations", "inner_iterations", "rel_residual", "solve_ms")}}),
+        flush=True)
 
 
 def profile_solve(args):

@@ -121,6 +121,7 @@ struct Handle {
     bool nn_enabled = true;    // cleared after repeated stagnation (fallback to multigrid)
     int fallbacks = 0;         // learned → multigrid fallbacks taken in the current solve
     int calib_mg = 0, calib_nn = 0;  // FCG iterations of the calibration solves (learned vs MG)
+    int nn_verdict = -1;       // judge's verdict on the current weights: -1 not judged, 0 off, 1 on
     int nn_level = 2;       // hierarchy level the network acts on
     DBuf mg_xs, mg_xk, mg_xt;  // FP32 fine-level scratch of the training data generator
 

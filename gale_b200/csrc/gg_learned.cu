@@ -515,6 +515,7 @@ void learned_set_weights(Handle& H, const float* w) {
     k_to_bf16<<<g(P), 256, 0, H.stream>>>(P, S.w32.as<float>(), S.wbf.as<__nv_bfloat16>());
     GG_CUDA(cudaStreamSynchronize(H.stream));
     H.nn_ready = true;
+    H.nn_verdict = -1;  // new weights: judge again
 }
 
 void learned_get_weights(Handle& H, float* w) {
@@ -699,6 +700,7 @@ int learned_train(Handle& H, const gg_learn_params& P, gg_learn_stats& st) {
     float ms = 0.f;
     GG_CUDA(cudaEventElapsedTime(&ms, H.ev0, H.ev1));
     H.nn_ready = true;
+    H.nn_verdict = -1;  // new weights: judge again
     st.samples = nsamp;
     st.loss_first = (float)first;
     st.loss_last = (float)last;

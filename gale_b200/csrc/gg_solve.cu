@@ -691,10 +691,14 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     };
     const double fnorm = sqrt(dot(H, nd, f, f));
     if (fnorm / sqrt((double)nfree) <= 1e-99) return GG_ERR_ZERO_FORCE;
-    if (prm.inner == GG_INNER_LEARNED_CG && learned_ready(H)) {
-        // the plain multigrid solve judges the learned one: both solve K e = f once in
-        // FP32; the learned correction stays on for this Uzawa solve only if it needs
-        // fewer flexible-CG iterations than multigrid alone
+    if (prm.inner == GG_INNER_LEARNED_CG && learned_ready(H) && H.nn_verdict == 0) {
+        // judged off for these weights: plain multigrid, no calibration cost
+        H.nn_enabled = false;
+        H.fallbacks = 1;
+    } else if (prm.inner == GG_INNER_LEARNED_CG && learned_ready(H) && H.nn_verdict < 0) {
+        // the plain multigrid solve judges the learned one, once per set of weights: both
+        // solve K e = f in FP32; the learned correction stays on only if it needs fewer
+        // flexible-CG iterations than multigrid alone
         int rc0 = mg_setup(H);
         if (rc0 != GG_OK) return rc0;
         learned_prepare(H);
@@ -715,6 +719,7 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
             H.nn_enabled = false;
             H.fallbacks++;
         }
+        H.nn_verdict = H.nn_enabled ? 1 : 0;
     }
     // STEP 1 (:553-565)
     if ((rc = inner(f, vstar, prm.tolerance)) != GG_OK) return fail("first inner solve (K u* = f)", rc);

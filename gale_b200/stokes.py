@@ -320,7 +320,11 @@ class StokesProblem:
         u = np.zeros(self.nnode * self.dim)
         p = np.zeros(self.nel) if p0 is None else f64(p0).copy()
         st = abi.UzawaStats()
-        self._check(self.lib.gg_uzawa_solve(self.h, C.byref(params), ptr(u), ptr(p), C.byref(st)))
+        rc = self.lib.gg_uzawa_solve(self.h, C.byref(params), ptr(u), ptr(p), C.byref(st))
+        if rc != 0:
+            err = GaleError(rc, self.lib.gg_last_error(self.h).decode())
+            err.stats = st.as_dict()  # how far the solve got
+            raise err
         return u, p, st.as_dict()
 
     def picard(self, picard: abi.PicardParams, params: abi.UzawaParams):
