@@ -134,7 +134,9 @@ def gale_arm(args):
         st_tr = G.train_learned(level=2, n_rhs=4, iters_per_rhs=6, epochs=40)
         learned = {"level": 2, "train_s": time.perf_counter() - t0, "samples": st_tr["samples"],
                    "loss_first": st_tr["loss_first"], "loss_last": st_tr["loss_last"]}
-    head = UzawaSolver(tolerance=1e-6, precision="mixed", inner=args.inner)
+    # the multigrid smoothing degree is a tuned parameter of this configuration (degree 3:
+    # 831 instead of 1242 inner iterations on 64³; the library default stays 2)
+    head = UzawaSolver(tolerance=1e-6, precision="mixed", inner=args.inner, smoothingDegree=args.smoothing_degree)
     plain = UzawaSolver(tolerance=1e-6, precision="fp64", inner="jacobi")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
@@ -185,7 +187,8 @@ def gale_arm(args):
         # accuracy-matched pair: both paths at the Uzawa rtol that brings them within ~1e-6
         # of that solution, one device-timed solve each (build included)
         t_ah, st_ah, (ua, pa) = timed(UzawaSolver(tolerance=args.accurate_rtol, precision="mixed", inner=args.inner,
-                                                  innerRtolFactor=0.01, maxIterations=5000), "mixed", 1, 0)
+                                                  innerRtolFactor=0.01, maxIterations=5000,
+                                                  smoothingDegree=args.smoothing_degree), "mixed", 1, 0)
         t_ap, st_ap, (uq, pq) = timed(UzawaSolver(tolerance=args.accurate_rtol, precision="fp64", inner="jacobi",
                                                   **deep), "fp64", 1, 0)
         accuracy = {
@@ -299,6 +302,7 @@ def gale_arm(args):
             "data": "synthetic (seeded; no dataset)",
             "config": {"workload": WORKLOAD, "elements": G.nel, "velocity_dofs": G.nnode * 3,
                        "points": G.np, "uzawa_rtol": 1e-6, "inner": args.inner,
+                       "smoothing_degree": args.smoothing_degree,
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replicas x{world}"},
             "plain_fp64_s": t_plain, "speedup_vs_plain_fp64": t_plain / t_head,
@@ -399,6 +403,7 @@ def main():
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--serial-sample", type=int, default=24)
     ap.add_argument("--accurate-rtol", type=float, default=1e-9)
+    ap.add_argument("--smoothing-degree", type=int, default=3, help="multigrid Chebyshev degree of the headline path")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

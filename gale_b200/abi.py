@@ -91,7 +91,7 @@ class UzawaParams(C.Structure):
         ("min_iterations", C.c_int32), ("use_absolute_tolerance", C.c_int32),
         ("use_preconditioner", C.c_int32), ("inner", C.c_int32), ("precision", C.c_int32),
         ("inner_rtol_factor", C.c_double), ("inner_max_iterations", C.c_int32),
-        ("reuse_pressure", C.c_int32), ("recycle_directions", C.c_int32),
+        ("reuse_pressure", C.c_int32), ("recycle_directions", C.c_int32), ("smoothing_degree", C.c_int32),
     ]
 
 

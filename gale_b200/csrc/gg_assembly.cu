@@ -20,6 +20,10 @@
 // range in chunks of 512.  Phase 1 (one thread per point, coalesced loads): rheology,
 // c_p, force weights → shared memory.  Phase 2 (one thread per element): sequential
 // sums in point order, i.e. the reference's summation order.
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
 
@@ -27,8 +31,14 @@ namespace gg {
 
 namespace {
 
-constexpr int kElemPerCta = 128;
-constexpr int kChunk = 512;
+// CTA shapes (elements per CTA = threads, points per shared-memory chunk) the autotuner
+// chooses from; the sums per element run in point order whatever the shape, so every
+// shape gives the same moments.
+struct BuildShape {
+    int epc, chunk;
+};
+constexpr BuildShape kShapes[] = {{64, 256}, {128, 256}, {128, 512}, {256, 512}};
+constexpr int kNumShapes = 4;
 
 template <typename R> __device__ __forceinline__ R r_exp(R x);
 template <> __device__ __forceinline__ double r_exp<double>(double x) { return exp(x); }
@@ -205,7 +215,7 @@ __device__ PointOut run_rheologies(const MeshK& mk, const gg_material& m, const 
     return out;
 }
 
-template <int DIM, typename R>
+template <int DIM, typename R, int kElemPerCta, int kChunk>
 __global__ void __launch_bounds__(kElemPerCta)
 k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
                 const double* __restrict__ xi_s, int64_t np_s, const int32_t* __restrict__ mat_s,
@@ -388,20 +398,87 @@ void upload_materials(Handle& H) {
                             cudaMemcpyHostToDevice, H.stream));
 }
 
-template <int DIM, typename R>
-static void launch_build(Handle& H, int prev, const double* pu, const double* pp, R* mom, R* kdiag,
-                         double* sdiag, double* f, bool outputs) {
+template <int DIM, typename R, int EPC, int CH>
+static void launch_shape(Handle& H, int prev, const double* pu, const double* pp, R* mom, R* kdiag, double* sdiag,
+                         double* f, bool outputs) {
     const int64_t nel = H.nel;
-    const int grid = (int)((nel + kElemPerCta - 1) / kElemPerCta);
+    const int grid = (int)((nel + EPC - 1) / EPC);
     const double* T = H.has_T ? H.T.as<double>() : nullptr;
     double g[3] = {H.force.g_hat[0], H.force.g_hat[1], H.force.g_hat[2]};
-    k_build_moments<DIM, R><<<grid, kElemPerCta, 0, H.stream>>>(
+    k_build_moments<DIM, R, EPC, CH><<<grid, EPC, 0, H.stream>>>(
         H.mk, nel, H.offsets.as<int32_t>(), H.xi_s.as<double>(), H.np_in, H.mat_s.as<int32_t>(),
         H.ps_s.as<double>(), T, pu, pp, prev, H.force.gravity, g[0], g[1], g[2], H.force.rayleigh,
         f ? 1 : 0, mom, kdiag, sdiag, f, outputs ? H.eta_s.as<double>() : nullptr,
         H.incr_s.as<double>(), H.yld_s.as<uint8_t>(), H.flag.as<int32_t>(), H.d_materials.as<gg_material>(),
         H.weights.mode == GG_WEIGHTS_DVC && H.dvc_valid ? H.w_s.as<double>() : nullptr);
     GG_CUDA(cudaGetLastError());
+}
+
+template <int DIM, typename R>
+static void launch_build_shape(int shape, Handle& H, int prev, const double* pu, const double* pp, R* mom, R* kdiag,
+                               double* sdiag, double* f, bool outputs) {
+    switch (shape) {
+        case 0: launch_shape<DIM, R, 64, 256>(H, prev, pu, pp, mom, kdiag, sdiag, f, outputs); break;
+        case 1: launch_shape<DIM, R, 128, 256>(H, prev, pu, pp, mom, kdiag, sdiag, f, outputs); break;
+        case 2: launch_shape<DIM, R, 128, 512>(H, prev, pu, pp, mom, kdiag, sdiag, f, outputs); break;
+        default: launch_shape<DIM, R, 256, 512>(H, prev, pu, pp, mom, kdiag, sdiag, f, outputs); break;
+    }
+}
+
+// Autotuner: the first build of a (device, dim, precision, points-per-element class) times
+// every CTA shape once on the real inputs (the atomically accumulated outputs are cleared
+// before each trial) and keeps the fastest for the rest of the process.
+struct BuildTuner {
+    std::mutex mu;
+    std::map<std::tuple<int, int, int, int>, int> best;
+};
+static BuildTuner& tuner() {
+    static BuildTuner t;
+    return t;
+}
+
+template <int DIM, typename R>
+static void launch_build(Handle& H, int prev, const double* pu, const double* pp, R* mom, R* kdiag,
+                         double* sdiag, double* f, bool outputs) {
+    int dev = 0;
+    GG_CUDA(cudaGetDevice(&dev));
+    const double ppe = H.nel ? (double)H.np_in / (double)H.nel : 0.0;
+    const int klass = ppe < 12 ? 0 : ppe < 24 ? 1 : ppe < 48 ? 2 : 3;
+    const auto key = std::make_tuple(dev, DIM, (int)sizeof(R), klass);
+    int shape = -1;
+    {
+        std::lock_guard<std::mutex> lk(tuner().mu);
+        auto it = tuner().best.find(key);
+        if (it != tuner().best.end()) shape = it->second;
+    }
+    const int64_t nd = H.ndof;
+    auto clear = [&]() {
+        GG_CUDA(cudaMemsetAsync(kdiag, 0, sizeof(R) * nd, H.stream));
+        if (f) GG_CUDA(cudaMemsetAsync(f, 0, sizeof(double) * nd, H.stream));
+    };
+    if (shape < 0) {
+        float best_ms = 1e30f;
+        int best = 2;
+        for (int k = 0; k < kNumShapes; k++) {
+            clear();
+            GG_CUDA(cudaEventRecord(H.ev0, H.stream));
+            launch_build_shape<DIM, R>(k, H, prev, pu, pp, mom, kdiag, sdiag, f, outputs);
+            GG_CUDA(cudaEventRecord(H.ev1, H.stream));
+            GG_CUDA(cudaEventSynchronize(H.ev1));
+            float ms = 0.f;
+            GG_CUDA(cudaEventElapsedTime(&ms, H.ev0, H.ev1));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = k;
+            }
+        }
+        shape = best;
+        std::lock_guard<std::mutex> lk(tuner().mu);
+        tuner().best[key] = shape;
+        clear();
+    }
+    H.build_shape[sizeof(R) == 4 ? 1 : 0] = shape;
+    launch_build_shape<DIM, R>(shape, H, prev, pu, pp, mom, kdiag, sdiag, f, outputs);
 }
 
 int build_operator(Handle& H, int precision, int prev, const double* d_prev_u,

@@ -108,6 +108,7 @@ struct Handle {
     DBuf mg_part, mg_dense; // power-iteration partials; FP64 columns of the coarsest operator
     int64_t coarse_n = 0;   // 0: no dense coarse solve (Chebyshev on the coarsest level)
     int mg_degree = 2;      // Chebyshev degree of the smoother
+    int build_shape[2] = {-1, -1};  // autotuned CTA shape of the FP64 / FP32 moment build
     // persistent multigrid FCG (gg_fused.cu): level table for the current hierarchy
     DBuf fused_tab, fused_part, fused_bar;
     std::vector<unsigned char> fused_host;

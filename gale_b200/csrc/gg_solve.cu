@@ -670,6 +670,17 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     const int64_t launches0 = H.kernel_launches;
     H.fallbacks = 0;
     H.nn_enabled = true;
+    {
+        // multigrid smoothing degree: captured V-cycles and the persistent kernel's phase
+        // table bake it in
+        int deg = prm.smoothing_degree > 0 ? prm.smoothing_degree : 2;
+        if (deg < 2 || deg > 4) return GG_ERR_INVALID;
+        if (deg != H.mg_degree) {
+            H.mg_degree = deg;
+            release_graphs(H);
+            H.fused_gen = -2;
+        }
+    }
     int64_t nfree = H.nfree;
     const double scaleq = sqrt((double)ne);
     int rc = GG_OK, it = 0;

@@ -171,9 +171,10 @@ def Mesh(dim, elements, minCoord=None, maxCoord=None) -> abi.MeshDesc:
 def UzawaSolver(tolerance=1e-5, maxIterations=1000, minIterations=1,
                 useAbsoluteTolerance=False, preconditioner=True, inner="jacobi",
                 precision="fp64", innerRtolFactor=0.1, innerMaxIterations=10000,
-                reusePressure=False, recycle=None) -> abi.UzawaParams:
+                reusePressure=False, recycle=None, smoothingDegree=0) -> abi.UzawaParams:
     """Stokes_SLE_UzawaSolver XML parameters (Stokes_SLE_UzawaSolver.cxx:241-264).
-    recycle (default: on for the mixed path) starts each inner solve from β u*_prev."""
+    recycle (default: on for the mixed path) starts each inner solve from β u*_prev;
+    smoothingDegree (2..4, 0 = 2) is the multigrid Chebyshev degree per level and sweep."""
     p = abi.UzawaParams()
     p.tolerance = tolerance
     p.max_iterations = maxIterations
@@ -187,6 +188,7 @@ def UzawaSolver(tolerance=1e-5, maxIterations=1000, minIterations=1,
     p.inner_max_iterations = innerMaxIterations
     p.reuse_pressure = int(reusePressure)
     p.recycle_directions = int(precision == "mixed" if recycle is None else recycle)
+    p.smoothing_degree = int(smoothingDegree)
     return p
 
 

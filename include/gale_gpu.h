@@ -150,6 +150,10 @@ typedef struct gg_uzawa_params {
     int32_t recycle_directions;   /* GG_PRECISION_MIXED only: start the inner solve of
                                      K u* = G s from β u*_prev (s = z + β s_prev); the
                                      inner stopping rule stays relative to ‖G s‖        */
+    int32_t smoothing_degree;     /* multigrid: Chebyshev degree of the pre- and post-
+                                     smoothing on every level, 2..4 (0: 2); the role of
+                                     PETScMGSolver's downIterations/upIterations
+                                     (PETScMGSolver.cxx:182-183)                         */
 } gg_uzawa_params;
 
 typedef struct gg_uzawa_stats {
