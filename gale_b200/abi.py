@@ -41,6 +41,8 @@ PRECISION_MIXED = 1
 INNER_JACOBI_CG = 0
 INNER_MG_CG = 1
 INNER_LEARNED_CG = 2
+INNER_LEARNED_JACOBI_CG = 3
+LEARN_BASE_MULTIGRID, LEARN_BASE_JACOBI = 0, 1
 
 MAX_RHEOLOGIES = 4
 MAX_MATERIALS = 16
@@ -124,7 +126,7 @@ class PicardStats(C.Structure):
 
 class LearnParams(C.Structure):
     _fields_ = [("level", C.c_int32), ("n_rhs", C.c_int32), ("iters_per_rhs", C.c_int32),
-                ("epochs", C.c_int32), ("lr", C.c_float), ("seed", C.c_int32)]
+                ("epochs", C.c_int32), ("lr", C.c_float), ("seed", C.c_int32), ("base", C.c_int32)]
 
 
 class LearnStats(C.Structure):

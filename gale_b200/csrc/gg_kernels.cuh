@@ -85,6 +85,8 @@ bool fused_fcg_enabled();
 
 // Learned coarse correction (gg_learned.cu)
 bool learned_ready(Handle& H);
+int learned_base(Handle& H);  // GG_LEARN_BASE_* of the current weights, −1 without a network
+void jacobi_precond(Handle& H, const float* r, float* z, const int32_t* done);
 void learned_prepare(Handle& H);
 void learned_correction(Handle& H, const float* r, float* z, const int32_t* done);
 int learned_set_level(Handle& H, int level);

@@ -273,6 +273,65 @@ __global__ void k_zero(int64_t n, float* __restrict__ a, const int32_t* __restri
 
 int g(int64_t n) { return grid_for(n, 256); }
 
+constexpr int kOmegaBlocks = 296;
+
+// ω = max(0, (d·r')/(dᵀA d)): the step along the learned direction d that minimises the
+// energy norm of the error left after z + ω d (r' = r − A z).  Per-block partials, the
+// last block to arrive sums them in block order; layout of w: [2·blocks partials][ω][pad]
+// then the arrival counter.
+__global__ void k_omega(int64_t n, const float* __restrict__ d, const float* __restrict__ r1,
+                        const float* __restrict__ ad, double* __restrict__ w, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    double num = 0.0, den = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        num += (double)d[i] * (double)r1[i];
+        den += (double)d[i] * (double)ad[i];
+    }
+    __shared__ double s_num[32], s_den[32];
+    __shared__ bool last;
+    for (int o = 16; o > 0; o >>= 1) {
+        num += __shfl_down_sync(0xffffffffu, num, o);
+        den += __shfl_down_sync(0xffffffffu, den, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_num[wid] = num;
+        s_den[wid] = den;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+            a += s_num[k];
+            b += s_den[k];
+        }
+        w[2 * blockIdx.x] = a;
+        w[2 * blockIdx.x + 1] = b;
+        __threadfence();
+        unsigned int* counter = reinterpret_cast<unsigned int*>(w + 2 * gridDim.x + 2);
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < (int)gridDim.x; k++) {
+        a += w[2 * k];
+        b += w[2 * k + 1];
+    }
+    w[2 * gridDim.x] = (b > 0.0 && a > 0.0) ? a / b : 0.0;
+    *reinterpret_cast<unsigned int*>(w + 2 * gridDim.x + 2) = 0u;
+}
+
+// z += ω d with ω from k_omega
+__global__ void k_axpy_omega(int64_t n, const double* __restrict__ omega, const float* __restrict__ d,
+                             float* __restrict__ z, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    const float w = (float)*omega;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        z[i] += w * d[i];
+}
+
 }  // namespace
 
 // restriction / prolongation kernels of gg_mg.cu
@@ -289,6 +348,8 @@ struct LearnedState {
     DBuf xin, h, pre, y, scale;                 // inference buffers (batch 1)
     DBuf t0, r0;                                // fine-level A z and r − A z
     int64_t gen = -1;                           // build generation of logeta
+    int base = GG_LEARN_BASE_MULTIGRID;         // preconditioner the weights correct
+    DBuf d0, ad0, wred;                         // fine correction d, A d, ω reduction scratch
 };
 
 LearnedState& learned(Handle& H) {
@@ -318,6 +379,10 @@ static void ensure_net(Handle& H, size_t level) {
     S.scale.ensure(sizeof(float) * 4);
     S.t0.ensure(sizeof(float) * H.ndof);
     S.r0.ensure(sizeof(float) * H.ndof);
+    S.d0.ensure(sizeof(float) * H.ndof);
+    S.ad0.ensure(sizeof(float) * H.ndof);
+    S.wred.ensure(sizeof(double) * (2 * kOmegaBlocks + 2) + 16);
+    GG_CUDA(cudaMemsetAsync(S.wred.p, 0, sizeof(double) * (2 * kOmegaBlocks + 2) + 16, H.stream));
     if (S.rl.size() != level + 1) {
         S.rl.clear();
         S.el.clear();
@@ -360,7 +425,7 @@ static void net_forward(Handle& H, int B, const float* xin, float* hbuf, float* 
     H.kernel_launches += 2;
 }
 
-// z += P_{0←L} N(R_{L←0} r): enqueued inside the captured inner iteration
+// z += ω P_{0←L} N(R_{L←0} r'), r' = r − A z: enqueued inside the captured inner iteration
 void learned_correction(Handle& H, const float* r, float* z, const int32_t* done) {
     LearnedState& S = learned(H);
     const size_t Lv = S.level;
@@ -382,17 +447,49 @@ void learned_correction(Handle& H, const float* r, float* z, const int32_t* done
     k_nn_output<<<g(N * dim), 256, 0, H.stream>>>(N, dim, H.mg[Lv]->bcmask, S.y.as<float>(), S.scale.as<float>(),
                                                   S.el[Lv]->as<float>(), done);
     H.kernel_launches += 2;
+    // d = P_{0←L} N(·) on the fine level
     for (size_t l = Lv; l >= 1; l--) {
-        float* dst = (l == 1) ? z : S.el[l - 1]->as<float>();
-        if (l > 1) {
-            k_zero<<<g(H.mg[l - 1]->ndof), 256, 0, H.stream>>>(H.mg[l - 1]->ndof, dst, done);
-            H.kernel_launches++;
-        }
+        float* dst = (l == 1) ? S.d0.as<float>() : S.el[l - 1]->as<float>();
+        k_zero<<<g(H.mg[l - 1]->ndof), 256, 0, H.stream>>>(H.mg[l - 1]->ndof, dst, done);
+        H.kernel_launches++;
         mg_prolong_add(H, l, S.el[l]->as<float>(), dst, done);
     }
+    // z += ω d with the energy-optimal ω ≥ 0, so the correction never raises the error
+    k_zero<<<g(H.ndof), 256, 0, H.stream>>>(H.ndof, S.ad0.as<float>(), done);
+    apply_K_ex<float>(L0.mk, L0.mom32, L0.bcmask, S.d0.as<float>(), S.ad0.as<float>(), nullptr, apply_grid(L0.nel),
+                      H.stream, done);
+    k_omega<<<kOmegaBlocks, 256, 0, H.stream>>>(H.ndof, S.d0.as<float>(), S.r0.as<float>(), S.ad0.as<float>(),
+                                                 S.wred.as<double>(), done);
+    k_axpy_omega<<<g(H.ndof), 256, 0, H.stream>>>(H.ndof, S.wred.as<double>() + 2 * kOmegaBlocks,
+                                                  S.d0.as<float>(), z, done);
+    H.kernel_launches += 4;
 }
 
 bool learned_ready(Handle& H) { return H.learned && H.nn_ready; }
+
+int learned_base(Handle& H) { return H.learned ? H.learned->base : -1; }
+
+namespace {
+// z = D⁻¹ r on the fine level (FP32 Jacobi diagonal, zero on BC rows)
+__global__ void k_jacobi_z(int64_t n, const float* __restrict__ invd, const float* __restrict__ r,
+                           float* __restrict__ z, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        z[i] = invd[i] * r[i];
+}
+// x += ω z
+__global__ void k_axpyw(int64_t n, float w, const float* __restrict__ z, float* __restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += w * z[i];
+}
+}  // namespace
+
+// z = D⁻¹ r: the plain Jacobi preconditioner, enqueued inside captured iterations
+void jacobi_precond(Handle& H, const float* r, float* z, const int32_t* done) {
+    const MGLevel& L0 = *H.mg[0];
+    k_jacobi_z<<<g(H.ndof), 256, 0, H.stream>>>(H.ndof, L0.invdiag.as<float>(), r, z, done);
+    H.kernel_launches++;
+}
 
 void learned_prepare(Handle& H) {
     if (!learned_ready(H)) return;
@@ -576,6 +673,12 @@ int learned_train(Handle& H, const gg_learn_params& P, gg_learn_stats& st) {
     const int dim = H.dim;
     const int64_t N = S.grid.n();
     const int64_t nd = H.ndof;
+    if (P.base != GG_LEARN_BASE_MULTIGRID && P.base != GG_LEARN_BASE_JACOBI)
+        return set_error(H, GG_ERR_INVALID, "learned base");
+    S.base = P.base;
+    const bool jac = S.base == GG_LEARN_BASE_JACOBI;
+    // damped Jacobi that advances the sampled iterates: ω = 1/λ_max(D⁻¹A)
+    const float omega = (float)(1.0 / H.mg[0]->lambda_max);
     learned_refresh(H);
     GG_CUDA(cudaEventRecord(H.ev0, H.stream));
     init_weights(H, (uint64_t)P.seed * 7919ull + 17ull);
@@ -599,26 +702,50 @@ int learned_train(Handle& H, const gg_learn_params& P, gg_learn_stats& st) {
     std::vector<uint8_t> bcL(N);
     GG_CUDA(cudaMemcpyAsync(bcL.data(), H.mg[S.level]->bcmask, N, cudaMemcpyDeviceToHost, H.stream));
     int samp = 0;
+    std::vector<float> ec;
     for (int j = 0; j < nrhs; j++) {
-        // right-hand side: the force vector, then G s for random pressures
-        if (j == 0) {
-            train_cast(H, H.f.as<double>(), b32, nd);
-        } else {
-            for (auto& v : s_host) v = nd01(rng);
-            GG_CUDA(cudaMemcpyAsync(H.qtmp.p, s_host.data(), sizeof(double) * H.nel, cudaMemcpyHostToDevice, H.stream));
-            apply_G(H, H.qtmp.as<double>(), H.ftmp.as<double>(), H.stream);
-            train_cast(H, H.ftmp.as<double>(), b32, nd);
+        if (jac) {
+            // Jacobi base: the error a coarse correction must remove lives in the coarse
+            // space -- x* = P e_L for a random level-L vector e_L, b = A x*
+            const MGLevel& LL = *H.mg[S.level];
+            ec.resize((size_t)dim * LL.nnode);
+            for (auto& v : ec) v = (float)nd01(rng);
+            GG_CUDA(cudaMemcpyAsync(S.el[S.level]->p, ec.data(), sizeof(float) * ec.size(), cudaMemcpyHostToDevice,
+                                    H.stream));
+            for (size_t l = S.level; l >= 1; l--) {
+                float* dst = (l == 1) ? xs : S.el[l - 1]->as<float>();
+                GG_CUDA(cudaMemsetAsync(dst, 0, sizeof(float) * (l == 1 ? nd : H.mg[l - 1]->ndof), H.stream));
+                mg_prolong_add(H, l, S.el[l]->as<float>(), dst, nullptr);
+            }
+            GG_CUDA(cudaMemsetAsync(zk, 0, sizeof(float) * nd, H.stream));
+            train_residual(H, zk, xs, rk);  // rk = −A x*
+            GG_CUDA(cudaMemsetAsync(b32, 0, sizeof(float) * nd, H.stream));
+            k_axpyw<<<g(nd), 256, 0, H.stream>>>(nd, -1.f, rk, b32);
         }
-        int its = 0;
-        rc = fcg_mg_solve(H, b32, xs, 1e-6, 2000, &its);
-        if (rc != GG_OK) return rc;
+        if (!jac) {
+            // multigrid base: right-hand sides the solver meets -- the force vector, then
+            // G s for random pressures, with x* from the multigrid solve
+            if (j == 0) {
+                train_cast(H, H.f.as<double>(), b32, nd);
+            } else {
+                for (auto& v : s_host) v = nd01(rng);
+                GG_CUDA(cudaMemcpyAsync(H.qtmp.p, s_host.data(), sizeof(double) * H.nel, cudaMemcpyHostToDevice,
+                                        H.stream));
+                apply_G(H, H.qtmp.as<double>(), H.ftmp.as<double>(), H.stream);
+                train_cast(H, H.ftmp.as<double>(), b32, nd);
+            }
+            int its = 0;
+            rc = fcg_mg_solve(H, b32, xs, 1e-6, 2000, &its);
+            if (rc != GG_OK) return rc;
+        }
         GG_CUDA(cudaMemsetAsync(xk, 0, sizeof(float) * nd, H.stream));
         for (int k = 0; k < kits; k++) {
-            // r = b − A x_k ; z = V(r) ; t = x* − x_k − z ; x_{k+1} = x_k + z
+            // r = b − A x_k ; z = M(r) (V-cycle or D⁻¹) ; t = x* − x_k − z
             train_residual(H, b32, xk, rk);
-            vcycle(H, 0, rk, zk, nullptr);
+            if (jac) jacobi_precond(H, rk, zk, nullptr);
+            else vcycle(H, 0, rk, zk, nullptr);
             train_target(H, xs, xk, zk, tk);
-            // input: the residual the V-cycle leaves, r' = r − A z (target t = A⁻¹ r');
+            // input: the residual the base preconditioner leaves, r' = r − A z (t = A⁻¹ r');
             // restricted to level L; target t injected to level L
             {
                 MGLevel& L0 = *H.mg[0];
@@ -646,7 +773,16 @@ int learned_train(Handle& H, const gg_learn_params& P, gg_learn_stats& st) {
                     if (!((bcL[n] >> c) & 1)) s += (double)th[c * N + n] * th[c * N + n];
             wts.push_back((float)(1.0 / (s > 1e-30 ? s : 1e-30)));
             samp++;
-            train_axpy(H, zk, xk);
+            if (jac) {
+                // the next sample four damped Jacobi steps on: a smoother, larger error
+                for (int q = 0; q < 4; q++) {
+                    train_residual(H, b32, xk, rk);
+                    jacobi_precond(H, rk, zk, nullptr);
+                    k_axpyw<<<g(nd), 256, 0, H.stream>>>(nd, omega, zk, xk);
+                }
+            } else {
+                train_axpy(H, zk, xk);  // x_{k+1} = x_k + V(r_k)
+            }
         }
     }
     GG_CUDA(cudaMemcpyAsync(Wt.p, wts.data(), sizeof(float) * nsamp, cudaMemcpyHostToDevice, H.stream));

@@ -539,6 +539,14 @@ static void ensure_solver_buffers(Handle& H, bool mixed) {
     init_scratch(H);
 }
 
+// The learned variant an inner mode asks for can run only with weights trained for the
+// same base preconditioner.
+static bool learned_usable(Handle& H, const gg_uzawa_params& prm) {
+    const int want = prm.inner == GG_INNER_LEARNED_CG ? GG_LEARN_BASE_MULTIGRID
+                   : prm.inner == GG_INNER_LEARNED_JACOBI_CG ? GG_LEARN_BASE_JACOBI : -1;
+    return want >= 0 && learned_ready(H) && learned_base(H) == want;
+}
+
 // x = K⁻¹ b (device FP64 vectors), stopping rule of the reference's inner KSP.
 int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* x, double rtol,
                 int maxit, int* iters, bool warm) {
@@ -587,13 +595,19 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
         return GG_OK;
     }
     const bool use_mg = prm.inner == GG_INNER_MG_CG || prm.inner == GG_INNER_LEARNED_CG;
-    if (use_mg) {
+    const bool learned_jac = prm.inner == GG_INNER_LEARNED_JACOBI_CG;
+    if (use_mg || learned_jac) {  // the learned Jacobi variant restricts through the levels
         int rc = mg_setup(H);
         if (rc != GG_OK) return rc;
     }
-    bool use_nn = prm.inner == GG_INNER_LEARNED_CG && learned_ready(H) && H.nn_enabled;
+    bool use_nn = learned_usable(H, prm) && H.nn_enabled;
     if (use_nn) learned_prepare(H);
     const double inner_rtol = use_mg ? 1e-4 : 1e-3;
+    // the base preconditioner of the learned variants (and their fallback)
+    auto base_pc = [&](const float* rr, float* zz, const int32_t* dn) {
+        if (learned_jac) jacobi_precond(H, rr, zz, dn);
+        else vcycle(H, 0, rr, zz, dn);
+    };
     // One FP32 sweep stops at inner_rtol or at sweep_cap iterations, whichever comes first;
     // a capped sweep still reduces the defect and the FP64 refinement below carries on from
     // it.  The cap keeps an FP32 solve that has hit its rounding floor (large viscosity
@@ -604,12 +618,13 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
         int it = 0;
         int rc;
         if (use_nn) {
-            // learned coarse correction added to the V-cycle; a stagnating solve (no
-            // convergence within kLearnedCap iterations) falls back to plain multigrid
-            constexpr int kLearnedCap = 40;
-            rc = run_fcg(H, "fcg_nn", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, std::min(maxit, kLearnedCap), &it,
-                         [&](const float* rr, float* zz, const int32_t* dn) {
-                             vcycle(H, 0, rr, zz, dn);
+            // learned coarse correction added to the base preconditioner; a stagnating solve
+            // (no convergence within the cap: 40 iterations over the V-cycle, twice the
+            // judge's plain Jacobi count over Jacobi) falls back to the base alone
+            const int cap = learned_jac ? std::max(2 * H.calib_mg, 100) : 40;
+            rc = run_fcg(H, learned_jac ? "fcg_jnn" : "fcg_nn", H.r32.as<float>(), H.e32.as<float>(), inner_rtol,
+                         std::min(maxit, cap), &it, [&](const float* rr, float* zz, const int32_t* dn) {
+                             base_pc(rr, zz, dn);
                              learned_correction(H, rr, zz, dn);
                          });
             if (rc != GG_OK) {
@@ -617,9 +632,12 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
                 total += it;
                 if (H.fallbacks >= 2) H.nn_enabled = false;  // stop trying for this handle's build
                 use_nn = H.nn_enabled;
-                rc = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it,
-                             [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+                rc = run_fcg(H, learned_jac ? "fcg_jac" : "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), inner_rtol,
+                             sweep_cap, &it, base_pc);
             }
+        } else if (learned_jac) {
+            // no usable network: the plain Jacobi flexible CG
+            rc = run_fcg(H, "fcg_jac", H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it, base_pc);
         } else if (use_mg) {
             rc = fused_fcg_enabled() ? run_fcg_fused(H, H.r32.as<float>(), H.e32.as<float>(), inner_rtol, sweep_cap, &it)
                                      : 1;
@@ -702,25 +720,32 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     };
     const double fnorm = sqrt(dot(H, nd, f, f));
     if (fnorm / sqrt((double)nfree) <= 1e-99) return GG_ERR_ZERO_FORCE;
-    if (prm.inner == GG_INNER_LEARNED_CG && learned_ready(H) && H.nn_verdict == 0) {
-        // judged off for these weights: plain multigrid, no calibration cost
+    if (learned_usable(H, prm) && H.nn_verdict == 0) {
+        // judged off for these weights: the base preconditioner alone, no calibration cost
         H.nn_enabled = false;
         H.fallbacks = 1;
-    } else if (prm.inner == GG_INNER_LEARNED_CG && learned_ready(H) && H.nn_verdict < 0) {
-        // the plain multigrid solve judges the learned one, once per set of weights: both
-        // solve K e = f in FP32; the learned correction stays on only if it needs fewer
-        // flexible-CG iterations than multigrid alone
+    } else if (learned_usable(H, prm) && H.nn_verdict < 0) {
+        // the plain solve judges the learned one, once per set of weights: both solve
+        // K e = f in FP32 with the base preconditioner (V-cycle or Jacobi), without and with
+        // the learned correction; it stays on only if it needs fewer flexible-CG iterations
+        const bool jac = prm.inner == GG_INNER_LEARNED_JACOBI_CG;
+        const double crtol = jac ? 1e-3 : 1e-4;
         int rc0 = mg_setup(H);
         if (rc0 != GG_OK) return rc0;
         learned_prepare(H);
+        auto base_pc = [&](const float* rr, float* zz, const int32_t* dn) {
+            if (jac) jacobi_precond(H, rr, zz, dn);
+            else vcycle(H, 0, rr, zz, dn);
+        };
         k_to_f32<<<grid_for(nd, 256), 256, 0, st>>>(nd, f, H.r32.as<float>());
         int it_mg = 0, it_nn = 0;
-        rc0 = run_fcg(H, "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), 1e-4, maxit, &it_mg,
-                      [&](const float* rr, float* zz, const int32_t* dn) { vcycle(H, 0, rr, zz, dn); });
+        rc0 = run_fcg(H, jac ? "fcg_jac" : "fcg_mg", H.r32.as<float>(), H.e32.as<float>(), crtol, maxit, &it_mg,
+                      base_pc);
         if (rc0 != GG_OK) return rc0;
-        rc0 = run_fcg(H, "fcg_nn", H.r32.as<float>(), H.e32.as<float>(), 1e-4, std::min(maxit, 40), &it_nn,
+        rc0 = run_fcg(H, jac ? "fcg_jnn" : "fcg_nn", H.r32.as<float>(), H.e32.as<float>(), crtol,
+                      std::min(maxit, jac ? std::max(2 * it_mg, 100) : 40), &it_nn,
                       [&](const float* rr, float* zz, const int32_t* dn) {
-                          vcycle(H, 0, rr, zz, dn);
+                          base_pc(rr, zz, dn);
                           learned_correction(H, rr, zz, dn);
                       });
         H.calib_mg = it_mg;

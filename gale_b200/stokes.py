@@ -181,8 +181,8 @@ def UzawaSolver(tolerance=1e-5, maxIterations=1000, minIterations=1,
     p.min_iterations = minIterations
     p.use_absolute_tolerance = int(useAbsoluteTolerance)
     p.use_preconditioner = int(preconditioner)
-    p.inner = {"jacobi": abi.INNER_JACOBI_CG, "mg": abi.INNER_MG_CG,
-               "learned": abi.INNER_LEARNED_CG}[inner]
+    p.inner = {"jacobi": abi.INNER_JACOBI_CG, "mg": abi.INNER_MG_CG, "learned": abi.INNER_LEARNED_CG,
+               "learned_jacobi": abi.INNER_LEARNED_JACOBI_CG}[inner]
     p.precision = {"fp64": abi.PRECISION_FP64, "mixed": abi.PRECISION_MIXED}[precision]
     p.inner_rtol_factor = innerRtolFactor
     p.inner_max_iterations = innerMaxIterations
@@ -368,8 +368,12 @@ class StokesProblem:
         return [(us[i], ps[i], st[i].as_dict()) for i in range(n)]
 
     # learned coarse correction
-    def train_learned(self, level=2, n_rhs=4, iters_per_rhs=6, epochs=60, lr=2e-3, seed=1):
-        p = abi.LearnParams(level, n_rhs, iters_per_rhs, epochs, lr, seed)
+    def train_learned(self, level=2, n_rhs=4, iters_per_rhs=6, epochs=60, lr=2e-3, seed=1, base="multigrid"):
+        """Train the coarse-correction network on pairs the solver generates for the current
+        operator; base "multigrid" (for inner="learned") or "jacobi" (inner="learned_jacobi")
+        is the preconditioner whose leftover error it learns to correct."""
+        p = abi.LearnParams(level, n_rhs, iters_per_rhs, epochs, lr, seed,
+                            {"multigrid": abi.LEARN_BASE_MULTIGRID, "jacobi": abi.LEARN_BASE_JACOBI}[base])
         st = abi.LearnStats()
         self._check(self.lib.gg_learned_train(self.h, C.byref(p), C.byref(st)))
         return st.as_dict()

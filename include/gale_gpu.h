@@ -132,8 +132,10 @@ enum {
 enum {
     GG_INNER_JACOBI_CG  = 0, /* PETSc -ksp_type cg -pc_type jacobi                     */
     GG_INNER_MG_CG      = 1, /* geometric multigrid V-cycle preconditioned CG          */
-    GG_INNER_LEARNED_CG = 2  /* MG + learned coarse correction, flexible CG; falls back
+    GG_INNER_LEARNED_CG = 2, /* MG + learned coarse correction, flexible CG; falls back
                                 to GG_INNER_MG_CG when the residual stagnates          */
+    GG_INNER_LEARNED_JACOBI_CG = 3 /* Jacobi + learned coarse correction, flexible CG;
+                                the plain Jacobi flexible CG judges and backs it up    */
 };
 
 typedef struct gg_uzawa_params {
@@ -194,7 +196,10 @@ typedef struct gg_learn_params {
     int32_t epochs;         /* Adam epochs                                                  */
     float   lr;             /* Adam learning rate                                           */
     int32_t seed;
+    int32_t base;           /* GG_LEARN_BASE_*: the preconditioner whose leftover error the
+                               network learns to correct                                     */
 } gg_learn_params;
+enum { GG_LEARN_BASE_MULTIGRID = 0, GG_LEARN_BASE_JACOBI = 1 };
 
 typedef struct gg_learn_stats {
     int32_t samples;

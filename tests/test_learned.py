@@ -106,3 +106,35 @@ def test_weights_transfer_between_instances():
     assert np.array_equal(GB.learned_weights(), wts)
     _, _, s = GB.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="learned"))
     assert s["rel_residual"] <= 1e-6
+
+
+def test_jacobi_base_judged_against_plain_jacobi():
+    """The network trained to correct the plain Jacobi preconditioner (the reference's
+    configured inner solver): the plain Jacobi flexible CG judges it, and whatever the
+    verdict the solve reaches the same solution at no more than the plain cost plus the
+    judge's two calibration solves."""
+    def prob():
+        w = workloads.creep_3d(n=32)
+        G = w.apply(StokesProblem(w.mesh))
+        G.locate()
+        G.build_operator("mixed")
+        return G
+    plain = prob()  # no network: inner="learned_jacobi" runs the plain Jacobi flexible CG
+    u0, p0, s0 = plain.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="learned_jacobi"))
+    G = prob()
+    st = G.train_learned(level=2, n_rhs=4, iters_per_rhs=6, epochs=60, base="jacobi")
+    assert st["loss_last"] < st["loss_first"]
+    u1, p1, s1 = G.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="learned_jacobi"))
+    assert s0["rel_residual"] <= 1e-6 and s1["rel_residual"] <= 1e-6
+    assert np.linalg.norm(u1 - u0) <= 1e-4 * np.linalg.norm(u0)
+    print(f"learned over Jacobi: inner iterations {s0['inner_iterations']} -> {s1['inner_iterations']}, "
+          f"judge {'kept it' if s1['fallbacks'] == 0 else 'switched it off'}")
+    if s1["fallbacks"] == 0:
+        assert s1["inner_iterations"] <= 1.05 * s0["inner_iterations"]
+    else:
+        assert s1["inner_iterations"] <= s0["inner_iterations"] + 400
+    # a network trained for the other base is not used by this mode
+    M = prob()
+    M.train_learned(level=2, epochs=5)
+    _, _, s2 = M.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="learned_jacobi"))
+    assert s2["inner_iterations"] == s0["inner_iterations"] and s2["fallbacks"] == 0
