@@ -400,7 +400,7 @@ def main():
     ap.add_argument("--max-outer", type=int, default=10000,
                     help="--config timestep: Uzawa maxIterations for the 1e6-contrast solve")
     ap.add_argument("--batch", type=int, default=512)
-    ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--workers", type=int, default=64)
     ap.add_argument("--serial-sample", type=int, default=24)
     ap.add_argument("--accurate-rtol", type=float, default=1e-9)
     ap.add_argument("--smoothing-degree", type=int, default=3, help="multigrid Chebyshev degree of the headline path")

