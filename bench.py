@@ -213,6 +213,12 @@ def gale_arm(args):
     alg_bytes = 2 * nu * pv + G.nel * 23 * pv
     achieved = alg_bytes / (ms.value * 1e-3) / 1e9
     peak, peak_kind = load_peaks()
+    # the plain FP64 Jacobi-CG iteration (the judge path) against the same peak: K reads p
+    # and writes Ap, the fused update reads Ap, r, x, p, diag and writes r, x, p (10·N_u·8)
+    # plus the FP64 moments (Nel·23·8); its time from the plain solve: solve time over the
+    # inner iterations (the outer Uzawa work is a few % of it)
+    cg_bytes = 10 * nu * 8 + G.nel * 23 * 8
+    cg_s = t_plain / max(1, st_plain["inner_iterations"])
     traffic = None
     prof = os.path.join(ROOT, "profiles", "k_apply_K_creep64.json")
     if os.path.exists(prof):
@@ -320,6 +326,10 @@ def gale_arm(args):
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": ms.value},
+            "roofline_plain_cg_iteration": {
+                "bound": "hbm", "achieved": cg_bytes / cg_s / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": cg_bytes / cg_s / 1e9 / peak, "algorithmic_bytes": cg_bytes, "s_per_iteration": cg_s,
+                "note": "upper bound on the time: the plain step includes build and outer Uzawa work"},
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -344,11 +354,23 @@ def cpu_baseline(w, inner_iterations, sample_its):
     t0 = time.perf_counter()
     _, its = P.inner_solve(b, 1e-30, sample_its)
     t_it = (time.perf_counter() - t0) / sample_its
+    # the same sample on one thread (a shorter CG run: the per-iteration cost is steady)
+    oracle.set_threads(1)
+    t0 = time.perf_counter()
+    P.assemble()
+    t_asm1 = time.perf_counter() - t0
+    its1 = max(5, sample_its // 6)
+    t0 = time.perf_counter()
+    P.inner_solve(b, 1e-30, its1)
+    t_it1 = (time.perf_counter() - t0) / its1
+    oracle.set_threads(cores)
     P.close()
     return {"value": t_asm + t_it * inner_iterations, "unit": "s", "cores": cores, "kind": "port",
             "sample": f"assembly + {sample_its} Jacobi-CG iterations timed, extrapolated to "
                       f"{inner_iterations} inner iterations of the plain FP64 Uzawa solve",
-            "assembly_s": t_asm, "s_per_cg_iteration": t_it}
+            "assembly_s": t_asm, "s_per_cg_iteration": t_it,
+            "single_thread": {"value": t_asm1 + t_it1 * inner_iterations, "assembly_s": t_asm1,
+                              "s_per_cg_iteration": t_it1, "sample_iterations": its1}}
 
 
 # Inner-iteration count of the FP64 Jacobi-CG Uzawa solve of creep_3d (seed 2024) to
