@@ -34,8 +34,8 @@ namespace {
 
 constexpr int kMinCoarse = 4;      // coarsen while every axis is even and ≥ 4 elements
 // … and the level has more dofs than this: the dense inverse of the coarsest level is
-// rebuilt at every operator build (Picard iterations included) by host Gauss–Jordan,
-// O(n³), so its size stays a few hundred dofs
+// rebuilt at every operator build (Picard iterations included) by device Gauss–Jordan,
+// n launches of O(n²) work, so its size stays a few hundred dofs
 constexpr int64_t kDenseStop = 400;
 
 __device__ __forceinline__ double tcoef(int a, int ap, double o) {
@@ -460,7 +460,7 @@ static double power_lambda(Handle& H, MGLevel& L) {
 }
 
 // Dense inverse of the coarsest level: columns K e_j from the matrix-free apply (FP64),
-// Gauss–Jordan with partial pivoting on the host.
+// then Gauss–Jordan on the device.
 // [A | I] with the BC rows and columns of A replaced by the identity (A symmetric:
 // column j of K was written to A + j·n)
 __global__ void k_gj_init(int64_t n, int64_t nnode, const uint8_t* __restrict__ bc, const double* __restrict__ A,
