@@ -182,6 +182,7 @@ ABI_FUNCTIONS = {
     "gg_last_error": ([_P], C.c_char_p),
     "gg_version": ([], C.c_char_p),
     "gg_set_velocity_bc": ([_P, C.POINTER(VelocityBC)], C.c_int),
+    "gg_set_velocity_bc_nodes": ([_P, _PU8, _PD], C.c_int),
     "gg_set_materials": ([_P, C.c_int32, C.POINTER(Material)], C.c_int),
     "gg_set_points": ([_P, C.c_int64, _PD, _PI32, _PD], C.c_int),
     "gg_set_temperature": ([_P, _PD], C.c_int),

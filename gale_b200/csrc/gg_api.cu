@@ -246,6 +246,33 @@ int gg_set_velocity_bc(gg_handle* h, const gg_velocity_bc* bc) {
     return GG_OK;
 }
 
+int gg_set_velocity_bc_nodes(gg_handle* h, const uint8_t* fixed, const double* values) {
+    if (!h || !fixed || !values) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    GG_TRY(h, {
+        const int dim = H.dim;
+        std::vector<uint8_t> mask(H.nnode, 0);
+        std::vector<double> val(H.ndof, 0.0);
+        int64_t nfixed = 0;
+        for (int64_t n = 0; n < H.nnode; n++) {
+            mask[n] = (uint8_t)(fixed[n] & ((1u << dim) - 1u));
+            for (int c = 0; c < dim; c++)
+                if ((mask[n] >> c) & 1) {
+                    val[(int64_t)c * H.nnode + n] = values[n * dim + c];
+                    nfixed++;
+                }
+        }
+        H.nfree = H.ndof - nfixed;
+        GG_CUDA(cudaMemcpyAsync(H.bcmask.p, mask.data(), H.nnode, cudaMemcpyHostToDevice, H.stream));
+        GG_CUDA(cudaMemcpyAsync(H.bcval.p, val.data(), sizeof(double) * H.ndof, cudaMemcpyHostToDevice, H.stream));
+        GG_CUDA(cudaStreamSynchronize(H.stream));
+        H.has_bc = true;
+        H.built = false;
+        gg::release_graphs(H);
+    })
+    return GG_OK;
+}
+
 int gg_set_materials(gg_handle* h, int32_t n, const gg_material* mats) {
     if (!h || !mats || n < 1 || n > GG_MAX_MATERIALS) return h ? gg::set_error(h->H, GG_ERR_INVALID, "material count") : GG_ERR_INVALID;
     for (int i = 0; i < n; i++)

@@ -243,6 +243,13 @@ class StokesProblem:
     def set_velocity_bc(self, bc):
         self._check(self.lib.gg_set_velocity_bc(self.h, C.byref(bc)))
 
+    def set_velocity_bc_nodes(self, fixed, values):
+        """Per-node velocity BCs (a condition function evaluated at the nodes): fixed
+        [nodes] with bit c = component c fixed, values [nodes, dim] node-major."""
+        self._bcf = np.ascontiguousarray(fixed, dtype=np.uint8)
+        self._bcv = f64(values)
+        self._check(self.lib.gg_set_velocity_bc_nodes(self.h, ptr(self._bcf, C.c_uint8), ptr(self._bcv)))
+
     def set_materials(self, mats: List[abi.Material]):
         arr = (abi.Material * len(mats))(*mats)
         self._check(self.lib.gg_set_materials(self.h, len(mats), arr))

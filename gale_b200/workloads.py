@@ -10,6 +10,7 @@ each configuration.  Every workload is deterministic for a given seed.
 * ``batch_sinkers``  uneven batch of 2D sinkers (n ∈ {32,48,64,96,128})
 * ``subduction_3d``  3D slab, 128×128×64, 27 per element
 * ``viscous_suite``  the 10×10 Gauss-swarm assembly of the reference's ViscousSuite
+* ``lid_driven_pic2d`` the reference's LidDrivenPIC2D regression model (20×20, PCDVC, 10 steps)
 """
 from __future__ import annotations
 
@@ -38,6 +39,7 @@ class Workload:
     uzawa: Any = None
     picard: Any = None
     meta: dict = field(default_factory=dict)
+    bc_nodes: Any = None  # (fixed [nodes] uint8, values [nodes, dim]) when BCs are functions
 
     @property
     def dim(self):
@@ -53,7 +55,10 @@ class Workload:
 
     def apply(self, prob):
         """Load the inputs into a StokesProblem (GPU) or an oracle problem (CPU)."""
-        prob.set_velocity_bc(self.bc)
+        if self.bc_nodes is not None:
+            prob.set_velocity_bc_nodes(*self.bc_nodes)
+        else:
+            prob.set_velocity_bc(self.bc)
         prob.set_materials(self.materials)
         prob.set_body_force(self.force)
         if self.temperature is not None:
@@ -192,6 +197,47 @@ def subduction_3d(nx=128, ny=64, nz=128, ppc=27, seed=5, tolerance=1e-6) -> Work
             RheologyMaterial([MaterialViscosity(1e-2)], density=1.0)]
     return Workload("subduction_3d", mesh, free_slip(3), mats, BodyForce(gravity=1.0), coords, material,
                     uzawa=UzawaSolver(tolerance=tolerance), meta={"ppc": ppc, "seed": seed})
+
+
+def partial_lid_top_layer(mesh: abi.MeshDesc, x: np.ndarray) -> np.ndarray:
+    """StgFEM_StandardConditionFunctions_PartialLid_TopLayer (StgFEM/plugins/
+    StandardConditionFunctions/StandardConditionFunctions.cxx:547-568): 1 where
+    min + margin < x < max − margin, else 0, margin = 1.1 × the minimum element separation."""
+    sep = min((mesh.max[d] - mesh.min[d]) / mesh.elements[d] for d in range(mesh.dim))
+    margin = sep * 1.1
+    return ((x < mesh.max[0] - margin) & (x > mesh.min[0] + margin)).astype(np.float64)
+
+
+def lid_driven_pic2d() -> Workload:
+    """PICellerator's regression model LidDrivenPIC2D (PICellerator/SysTest/RegressionTests/
+    LidDrivenPIC2D.xml with lidDrivenVelocityBCs.xml and the PIC_Components it includes):
+    2D unit square, 20×20 Q1-P0 elements, one material of viscosity 1
+    (IsoviscousStressTensorTerm, no body force), 36 points per cell from
+    SpaceFillerParticleLayout, PCDVC weights (resolution 10, lowerT 0.6, upperT 25,
+    maxDeletions 3, maxSplits 3), Uzawa tolerance 1e-5 / maxIterations 5000, RK2 advection,
+    10 time steps.  BCs: vy = 0 on the bottom, vx = 0 on the left and right walls,
+    vx = PartialLid_TopLayer(x) and vy = 0 on the top."""
+    mesh = Mesh(2, (20, 20), (0.0, 0.0), (1.0, 1.0))
+    from .layouts import space_filler
+    coords = space_filler(mesh, 36)
+    nodes = node_coords(mesh)
+    nx = mesh.elements[0] + 1
+    ix = np.arange(nodes.shape[0]) % nx
+    iy = np.arange(nodes.shape[0]) // nx
+    fixed = np.zeros(nodes.shape[0], dtype=np.uint8)
+    values = np.zeros((nodes.shape[0], 2))
+    fixed[iy == 0] |= 2                         # bottom: vy
+    fixed[(ix == 0) | (ix == nx - 1)] |= 1      # left, right: vx
+    top = iy == mesh.elements[1]
+    fixed[top] |= 3                             # top: vx (function), vy
+    values[top, 0] = partial_lid_top_layer(mesh, nodes[top, 0])
+    mats = [RheologyMaterial([MaterialViscosity(1.0)])]
+    return Workload("lid_driven_pic2d", mesh, abi.VelocityBC(), mats, BodyForce(), coords,
+                    np.zeros(coords.shape[0], dtype=np.int32),
+                    uzawa=UzawaSolver(tolerance=1e-5, maxIterations=5000),
+                    bc_nodes=(fixed, values),
+                    meta={"steps": 10, "order": 2, "weights_resolution": 10,
+                          "pcdvc": dict(upperT=25.0, lowerT=0.6, maxSplits=3, maxDeletions=3)})
 
 
 def viscous_suite(rheology: str):

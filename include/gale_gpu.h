@@ -224,6 +224,12 @@ GG_API const char* gg_version(void);
  * StgFEM/Discretisation/src/FeVariable.cxx) as consumed by __StiffnessMatrix_NewAssemble
  * (StgFEM/SLE/SystemSetup/src/StiffnessMatrix.cxx:2091-2143).                          */
 GG_API int  gg_set_velocity_bc(gg_handle* h, const gg_velocity_bc* bc);
+/* Velocity BCs per node: a VariableCondition whose values come from a condition function
+ * evaluated at the nodes by the host (the "func" entries of a WallVC, e.g.
+ * StgFEM_StandardConditionFunctions_PartialLid_TopLayer, StgFEM/plugins/
+ * StandardConditionFunctions/StandardConditionFunctions.cxx:547-568).  fixed: [nodes],
+ * bit c = component c fixed; values: [nodes*dim] node-major, read on fixed components. */
+GG_API int  gg_set_velocity_bc_nodes(gg_handle* h, const uint8_t* fixed, const double* values);
 /* Material table: RheologyMaterial + its Rheology_Register
  * (Underworld/Rheology/src/Rheology_Register.cxx:70-86), density/alpha of
  * BuoyancyForceTerm (PICellerator/Utils/src/BuoyancyForceTerm.cxx:414-530).           */

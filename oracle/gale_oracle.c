@@ -398,6 +398,23 @@ int or_set_velocity_bc(or_problem* P, const gg_velocity_bc* bc) {
     return GG_OK;
 }
 
+/* Per-node velocity BCs: a VariableCondition whose values come from a condition function
+ * evaluated at the nodes (VariableCondition "func" entries, e.g.
+ * StgFEM_StandardConditionFunctions_PartialLid_TopLayer, StgFEM/plugins/
+ * StandardConditionFunctions/StandardConditionFunctions.cxx:547-568).  fixed[n] bit c:
+ * component c fixed; values [nnode*dim], read on fixed components only. */
+int or_set_velocity_bc_nodes(or_problem* P, const uint8_t* fixed, const double* values) {
+    mesh_t* M = &P->M;
+    if (!fixed || !values) return fail(GG_ERR_INVALID, "null BC arrays");
+    for (int64_t n = 0; n < M->nnode; n++) {
+        P->bcmask[n] = (uint8_t)(fixed[n] & ((1u << M->dim) - 1u));
+        for (int c = 0; c < M->dim; c++)
+            P->bcval[n * M->dim + c] = (P->bcmask[n] >> c) & 1 ? values[n * M->dim + c] : 0.0;
+    }
+    P->assembled = 0;
+    return GG_OK;
+}
+
 int or_set_materials(or_problem* P, int32_t n, const gg_material* mats) {
     if (n < 1 || n > GG_MAX_MATERIALS) return fail(GG_ERR_INVALID, "material count");
     P->nmat = n;

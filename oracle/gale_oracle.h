@@ -37,6 +37,7 @@ or_problem* or_create(const gg_mesh_desc* m);
 void or_destroy(or_problem* P);
 int  or_set_threads(int n);
 int  or_set_velocity_bc(or_problem* P, const gg_velocity_bc* bc);
+int  or_set_velocity_bc_nodes(or_problem* P, const uint8_t* fixed, const double* values);
 int  or_set_materials(or_problem* P, int32_t n, const gg_material* mats);
 int  or_set_temperature(or_problem* P, const double* T);
 int  or_set_body_force(or_problem* P, const gg_body_force* f);

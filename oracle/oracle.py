@@ -34,6 +34,7 @@ _SIG = {
     "or_destroy": ([_P], None),
     "or_set_threads": ([C.c_int], C.c_int),
     "or_set_velocity_bc": ([_P, C.POINTER(abi.VelocityBC)], C.c_int),
+    "or_set_velocity_bc_nodes": ([_P, _PU8, _PD], C.c_int),
     "or_set_materials": ([_P, C.c_int32, C.POINTER(abi.Material)], C.c_int),
     "or_set_temperature": ([_P, _PD], C.c_int),
     "or_set_body_force": ([_P, C.POINTER(abi.BodyForce)], C.c_int),
@@ -154,6 +155,12 @@ class OracleProblem:
 
     def set_velocity_bc(self, bc):
         _check(lib().or_set_velocity_bc(self.h, C.byref(bc)))
+
+    def set_velocity_bc_nodes(self, fixed, values):
+        """fixed [nodes] (bit c: component c fixed), values [nodes, dim] node-major."""
+        self._bcf = np.ascontiguousarray(fixed, dtype=np.uint8)
+        self._bcv = f64(values)
+        _check(lib().or_set_velocity_bc_nodes(self.h, ptr(self._bcf, C.c_uint8), ptr(self._bcv)))
 
     def set_materials(self, mats):
         arr = (abi.Material * len(mats))(*mats)
