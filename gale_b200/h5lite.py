@@ -13,7 +13,9 @@ symbol tables (a version-1 B-tree of symbol-table nodes plus a local heap) and v
 object headers.  This module reads exactly that: groups, datasets with contiguous, compact
 or chunked (optionally deflate-compressed) storage, fixed-point and IEEE floating-point
 element types, and attributes.  It writes the same subset (superblock 0, one root group,
-contiguous datasets, scalar or array attributes), which the HDF5 library itself reads.
+contiguous datasets, array attributes) with the objects, message versions and field values
+that the HDF5 1.8 library wrote into the reference's checkpoint files, so that Gale reads them
+back (`FeVariable_ReadFromFile`, `SwarmDump`'s reader).
 
 The layouts follow the published HDF5 File Format Specification (version 2.0 of the
 document; superblock 0, object header 1, message types 0x01, 0x03, 0x05, 0x08, 0x0B,
@@ -330,3 +332,138 @@ def read(path) -> Dict[str, np.ndarray]:
     """Every dataset of the root group of `path` as {name: array}."""
     f = File(path)
     return {k: f[k] for k in f.keys() if not isinstance(f[k], File)}
+
+
+# ---------------------------------------------------------------------------- writing
+
+_GROUP_LEAF_K = 4        # symbol-table node holds 2K entries
+_GROUP_INTERNAL_K = 16   # B-tree node holds 2K children
+_HEAP_FREE_NULL = 1      # the library's "no free block" marker in a local heap
+
+
+def _u(v: int, n: int) -> bytes:
+    return int(v).to_bytes(n, "little")
+
+
+def _pad8(b: bytes) -> bytes:
+    return b + bytes((8 - len(b) % 8) % 8)
+
+
+def _dtype_msg(dt: np.dtype) -> bytes:
+    """Datatype message (version 1) of a fixed-point or IEEE floating-point numpy type."""
+    big = dt.byteorder == ">" or (dt.byteorder == "=" and np.little_endian is False)
+    if dt.kind == "f":
+        prec = dt.itemsize * 8
+        exp_loc, exp_size, man_size, bias = {4: (23, 8, 23, 127), 8: (52, 11, 52, 1023)}[dt.itemsize]
+        bits = bytes([0x20 | (1 if big else 0), prec - 1, 0])  # normalisation: implied msb; sign bit
+        props = _u(0, 2) + _u(prec, 2) + bytes([exp_loc, exp_size, 0, man_size]) + _u(bias, 4)
+        return bytes([0x11]) + bits + _u(dt.itemsize, 4) + props
+    if dt.kind in "iu":
+        bits = bytes([(1 if big else 0) | (0x08 if dt.kind == "i" else 0), 0, 0])
+        return bytes([0x10]) + bits + _u(dt.itemsize, 4) + _u(0, 2) + _u(dt.itemsize * 8, 2)
+    raise H5Error(f"numpy type {dt} is outside the writable subset")
+
+
+def _space_msg(shape) -> bytes:
+    """Dataspace message version 1, no maximum dimensions."""
+    return bytes([1, len(shape), 0, 0]) + bytes(4) + b"".join(_u(d, 8) for d in shape)
+
+
+def _message(mtype: int, body: bytes, flags: int = 0) -> bytes:
+    body = _pad8(body)
+    return _u(mtype, 2) + _u(len(body), 2) + bytes([flags]) + bytes(3) + body
+
+
+def _header(messages: List[bytes]) -> bytes:
+    body = b"".join(messages)
+    return bytes([1, 0]) + _u(len(messages), 2) + _u(1, 4) + _u(len(body), 4) + bytes(4) + body
+
+
+def _attribute(name: str, value: np.ndarray) -> bytes:
+    value = np.atleast_1d(np.asarray(value))
+    nm = name.encode() + b"\x00"
+    dtm, spm = _dtype_msg(value.dtype), _space_msg(value.shape)
+    body = (bytes([1, 0]) + _u(len(nm), 2) + _u(len(dtm), 2) + _u(len(spm), 2)
+            + _pad8(nm) + _pad8(dtm) + _pad8(spm) + value.tobytes())
+    return _message(0x0C, body)
+
+
+def write(path: str, datasets: Dict[str, np.ndarray], attrs: Optional[Dict[str, np.ndarray]] = None) -> None:
+    """Write an HDF5 file (superblock 0) whose root group holds `datasets` (contiguous,
+    numpy dtype and shape kept) and `attrs` as root-group attributes.  At most 8 datasets
+    (one symbol-table node), which covers every checkpoint file of the reference."""
+    names = sorted(datasets, key=lambda k: k.encode())
+    if len(names) > 2 * _GROUP_LEAF_K:
+        raise H5Error("more datasets than one symbol-table node holds")
+    arrays = {k: np.ascontiguousarray(datasets[k]) for k in names}
+    # local heap data: the empty name at offset 0, then each name, 8-byte padded
+    heap_data = bytearray(8)
+    name_off = {}
+    for k in names:
+        name_off[k] = len(heap_data)
+        heap_data += _pad8(k.encode() + b"\x00")
+    # fixed-size pieces
+    SB = 96
+    root_msgs_len = len(_message(0x11, bytes(16))) + sum(
+        len(_attribute(a, v)) for a, v in (attrs or {}).items())
+    root_hdr_len = 16 + root_msgs_len
+    heap_hdr_len = 32
+    btree_len = 24 + 8 * (2 * _GROUP_INTERNAL_K + 1) + 8 * (2 * _GROUP_INTERNAL_K)
+    snod_len = 8 + 40 * 2 * _GROUP_LEAF_K
+
+    def ds_header(arr, addr):
+        return _header([
+            _message(0x05, bytes([2, 2, 2, 1]) + _u(0, 4), flags=1),      # fill value: none
+            _message(0x03, _dtype_msg(arr.dtype), flags=1),
+            _message(0x01, _space_msg(arr.shape)),
+            _message(0x08, bytes([3, 1]) + _u(addr, 8) + _u(arr.nbytes, 8)),  # contiguous
+        ])
+
+    a_root = SB
+    a_heap = a_root + root_hdr_len
+    a_heap_data = a_heap + heap_hdr_len
+    a_btree = a_heap_data + len(heap_data)
+    a_snod = a_btree + btree_len
+    a = a_snod + snod_len
+    a_hdr = {}
+    for k in names:
+        a_hdr[k] = a
+        a += len(ds_header(arrays[k], 0))
+    a_raw = {}
+    for k in names:
+        a = (a + 7) // 8 * 8
+        a_raw[k] = a
+        a += arrays[k].nbytes
+    eof = a
+
+    out = bytearray()
+    # superblock 0 + root group symbol-table entry (cache type 1: B-tree and heap addresses)
+    out += SIGNATURE + bytes([0, 0, 0, 0, 0, 8, 8, 0]) + _u(_GROUP_LEAF_K, 2) + _u(_GROUP_INTERNAL_K, 2)
+    out += _u(0, 4) + _u(0, 8) + _u(UNDEF, 8) + _u(eof, 8) + _u(UNDEF, 8)
+    out += _u(0, 8) + _u(a_root, 8) + _u(1, 4) + _u(0, 4) + _u(a_btree, 8) + _u(a_heap, 8)
+    assert len(out) == SB
+    msgs = [_message(0x11, _u(a_btree, 8) + _u(a_heap, 8))]
+    msgs += [_attribute(k, v) for k, v in (attrs or {}).items()]
+    out += _header(msgs)
+    assert len(out) == a_heap
+    out += b"HEAP" + bytes([0, 0, 0, 0]) + _u(len(heap_data), 8) + _u(_HEAP_FREE_NULL, 8) + _u(a_heap_data, 8)
+    out += heap_data
+    assert len(out) == a_btree
+    bt = bytearray(b"TREE" + bytes([0, 0]) + _u(1 if names else 0, 2) + _u(UNDEF, 8) + _u(UNDEF, 8))
+    bt += _u(0, 8) + _u(a_snod, 8) + _u(name_off[names[-1]] if names else 0, 8)
+    bt += bytes(btree_len - len(bt))
+    out += bt
+    sn = bytearray(b"SNOD" + bytes([1, 0]) + _u(len(names), 2))
+    for k in names:
+        sn += _u(name_off[k], 8) + _u(a_hdr[k], 8) + _u(0, 4) + _u(0, 4) + bytes(16)
+    sn += bytes(snod_len - len(sn))
+    out += sn
+    for k in names:
+        assert len(out) == a_hdr[k]
+        out += ds_header(arrays[k], a_raw[k])
+    for k in names:
+        out += bytes(a_raw[k] - len(out))
+        out += arrays[k].tobytes()
+    assert len(out) == eof
+    with open(path, "wb") as f:
+        f.write(bytes(out))

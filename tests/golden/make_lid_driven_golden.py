@@ -34,6 +34,7 @@ def load(ref_root: str) -> dict:
         "current_time": tim["currentTime"],
         "dt": tim["Dt"],
         "vertices": msh["vertices"],
+        "connectivity": msh["connectivity"],
         "mesh_resolution": vel.attrs()["mesh resolution"],
         "swarm_particle_count": swm.attrs()["Swarm Particle Count"],
     }
