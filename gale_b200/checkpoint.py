@@ -14,8 +14,10 @@ Gale checkpoints step n as one HDF5 file per object in the output directory:
   "/connectivity", with each element's nodes in Gale's element order except that nodes 2
   and 3 (and 6 and 7) are swapped, so that every face runs counter-clockwise.
 
-`save` writes exactly those objects from this library's arrays; `load` reads them (Gale's
-own files included) back as numpy arrays.
+`save` writes exactly those objects from this library's arrays; `load` reads them back as
+numpy arrays, Gale's own files included, in the current format (version 2) and in the older
+version 1 (no attributes, the node number in column 0 of each field row, swarm variables
+named "<swarm>-<variable>").
 """
 from __future__ import annotations
 
@@ -100,21 +102,42 @@ def save(directory: str, step: int, mesh: abi.MeshDesc, u: np.ndarray, p: np.nda
     return paths
 
 
+def _rows(f: "h5lite.File", key: str) -> np.ndarray:
+    """Rows of a field dataset.  Version 2 files (root attribute "checkpoint file version")
+    hold one row per node in node order; version 1 files (no attributes,
+    FeVariable.cxx:2236-2240) put the global node number in column 0."""
+    data = f[key]
+    if "checkpoint file version" in f.attrs():
+        return data
+    order = np.argsort(data[:, 0], kind="stable")
+    return data[order, 1:]
+
+
+def _swarm_var(f: "h5lite.File", name: str) -> np.ndarray:
+    """Swarm variable `name`; older dumps prefix it with the swarm's name ("materialSwarm-")."""
+    for k in f.keys():
+        if k == name or k.endswith("-" + name):
+            return f[k]
+    raise KeyError(name)
+
+
 def load(directory: str, step: int) -> Dict[str, np.ndarray]:
-    """Read a checkpoint (this library's or Gale's) as flat arrays: velocity [nodes, dim],
-    pressure [elements], positions, material_index, current_time, dt, vertices,
-    connectivity, mesh_resolution."""
+    """Read a checkpoint (this library's or Gale's, version 1 or 2) as flat arrays: velocity
+    [nodes, dim], pressure [elements], positions, material_index, current_time, dt,
+    vertices, connectivity (None in version 1) and mesh_resolution (None in version 1)."""
     tag = f"{step:05d}"
     f = {k: h5lite.File(os.path.join(directory, f"{k}.{tag}.h5"))
          for k in ("VelocityField", "PressureField", "materialSwarm", "timeInfo", "Mesh")}
+    mesh = f["Mesh"]
+    v2 = "vertices" in mesh.keys()
     return {
-        "velocity": f["VelocityField"]["data"],
-        "pressure": f["PressureField"]["data"].ravel(),
-        "positions": f["materialSwarm"]["Position"],
-        "material_index": f["materialSwarm"]["MaterialIndex"].ravel(),
+        "velocity": _rows(f["VelocityField"], "data"),
+        "pressure": _rows(f["PressureField"], "data").ravel(),
+        "positions": _swarm_var(f["materialSwarm"], "Position"),
+        "material_index": _swarm_var(f["materialSwarm"], "MaterialIndex").ravel(),
         "current_time": float(f["timeInfo"]["currentTime"][0]),
         "dt": float(f["timeInfo"]["Dt"][0]),
-        "vertices": f["Mesh"]["vertices"],
-        "connectivity": f["Mesh"]["connectivity"],
-        "mesh_resolution": f["VelocityField"].attrs()["mesh resolution"],
+        "vertices": mesh["vertices"] if v2 else _rows(mesh, "data"),
+        "connectivity": mesh["connectivity"] if v2 else None,
+        "mesh_resolution": f["VelocityField"].attrs().get("mesh resolution"),
     }

@@ -11,6 +11,7 @@ each configuration.  Every workload is deterministic for a given seed.
 * ``subduction_3d``  3D slab, 128×128×64, 27 per element
 * ``viscous_suite``  the 10×10 Gauss-swarm assembly of the reference's ViscousSuite
 * ``lid_driven_pic2d`` the reference's LidDrivenPIC2D regression model (20×20, PCDVC, 10 steps)
+* ``rayleigh_taylor_benchmark`` the reference's RayleighTaylorBenchmark regression model (64×64)
 """
 from __future__ import annotations
 
@@ -236,6 +237,38 @@ def lid_driven_pic2d() -> Workload:
                     np.zeros(coords.shape[0], dtype=np.int32),
                     uzawa=UzawaSolver(tolerance=1e-5, maxIterations=5000),
                     bc_nodes=(fixed, values),
+                    meta={"steps": 10, "order": 2, "weights_resolution": 10,
+                          "pcdvc": dict(upperT=25.0, lowerT=0.6, maxSplits=3, maxDeletions=3)})
+
+
+def below_cosine_plane(coords: np.ndarray, offset=0.5, amplitude=0.1, wavelength=2 * np.pi,
+                       phase=0.0) -> np.ndarray:
+    """Stg_Shape BelowCosinePlane (StgDomain/Shape/src/BelowCosinePlane.cxx:196-213) with no
+    centre or rotation: inside where y < offset + amplitude·cos(2πx / wavelength + phase)."""
+    x, y = coords[:, 0], coords[:, 1]
+    return y < offset + amplitude * np.cos((2 * np.pi * x / wavelength) + phase)
+
+
+def rayleigh_taylor_benchmark() -> Workload:
+    """Underworld's regression model RayleighTaylorBenchmark (Underworld/SysTest/
+    RegressionTests/RayleighTaylorBenchmark.xml on BaseApps/RayleighTaylor.xml and
+    LidDrivenPIC.xml; van Keken et al. 1997): 64×64 Q1-P0 elements on [0, 0.9142]×[0, 1],
+    a light layer (density 0, viscosity 1) below y = 0.2 + 0.02 cos(2πx/1.8284) under a
+    background of density 1 and viscosity 1, gravity 1 (BuoyancyForceTerm), free-slip sides
+    and no-slip top and bottom, 20 points per cell from SpaceFillerParticleLayout, PCDVC
+    weights (resolution 10, lowerT 0.6, upperT 25, maxDeletions 3, maxSplits 3), Uzawa
+    tolerance 1e-5, RK2 advection.  Materials are set by shape in material order (the light
+    layer, defined second, wins where both shapes hold)."""
+    mesh = Mesh(2, (64, 64), (0.0, 0.0), (0.9142, 1.0))
+    from .layouts import space_filler
+    coords = space_filler(mesh, 20)
+    material = below_cosine_plane(coords, offset=0.2, amplitude=0.02, wavelength=1.8284,
+                                  phase=0.0).astype(np.int32)
+    mats = [RheologyMaterial([MaterialViscosity(1.0)], density=1.0),
+            RheologyMaterial([MaterialViscosity(1.0)], density=0.0)]
+    bc = VelocityBC(bottom={"vx": 0, "vy": 0}, top={"vx": 0, "vy": 0}, left={"vx": 0}, right={"vx": 0})
+    return Workload("rayleigh_taylor_benchmark", mesh, bc, mats, BodyForce(gravity=1.0), coords, material,
+                    uzawa=UzawaSolver(tolerance=1e-5, maxIterations=5000),
                     meta={"steps": 10, "order": 2, "weights_resolution": 10,
                           "pcdvc": dict(upperT=25.0, lowerT=0.6, maxSplits=3, maxDeletions=3)})
 
