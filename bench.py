@@ -220,7 +220,7 @@ def gale_arm(args):
     cg_bytes = 10 * nu * 8 + G.nel * 23 * 8
     cg_s = t_plain / max(1, st_plain["inner_iterations"])
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "k_apply_K_creep64.json")
+    prof = os.path.join(ROOT, "profiles", "k_apply_K_small_creep64.json")
     if os.path.exists(prof):
         traffic = json.load(open(prof)).get("dram_bytes_per_launch")
 
@@ -322,7 +322,7 @@ def gale_arm(args):
             "iterations": {"headline": {k: st_head[k] for k in ("outer_iterations", "inner_iterations")},
                            "plain_fp64": {k: st_plain[k] for k in ("outer_iterations", "inner_iterations")}},
             "gpu_launches": int(st_head["kernel_launches"]) * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_apply_K<3,float> (matrix-free K apply, FP32)",
+            "roofline": {"bound": "hbm", "kernel": "k_apply_K_small<3> (matrix-free K apply, FP32)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": ms.value},
@@ -623,7 +623,7 @@ def profile_apply(args):
     G.build_operator("mixed")
     ms = C.c_double(0)
     G._check(G.lib.gg_time_apply(G.h, abi.PRECISION_MIXED, max(1, args.profile_apply), C.byref(ms)))
-    print(json.dumps({"k_apply_K<3,float>_us": ms.value * 1e3, "reps": args.profile_apply}))
+    print(json.dumps({"k_apply_K_small<3>_us": ms.value * 1e3, "reps": args.profile_apply}))
 
 
 if __name__ == "__main__":

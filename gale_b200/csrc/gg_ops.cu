@@ -30,9 +30,31 @@ k_apply_K(MeshK mk, const R* __restrict__ mom, const uint8_t* __restrict__ bcmas
     }
 }
 
+// The FP32 apply without the energy: 128-thread blocks (32 × 2 × 2 elements in 3D, 32 × 4
+// in 2D), four per SM.  Blocks half the size start and finish at staggered times, so one
+// block's gathers overlap another's arithmetic more than with 256-thread blocks (64³:
+// 12.3 µs against 13.1 µs per launch).
+template <int DIM>
+__global__ void __launch_bounds__(128, 4)
+k_apply_K_small(MeshK mk, const float* __restrict__ mom, const uint8_t* __restrict__ bcmask,
+                const float* __restrict__ x, float* __restrict__ y, const int32_t* __restrict__ done) {
+    if (done && *done) return;
+    apply_tiles<DIM, float, 0, false, DIM == 3 ? 2 : 4, DIM == 3 ? 2 : 1>(mk, mom, bcmask, x, y, blockIdx.x, gridDim.x);
+}
+
 template <typename R>
 void apply_K_ex(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
                 double* energy_part, int grid, cudaStream_t st, const int32_t* done) {
+    if constexpr (sizeof(R) == 4) {
+        if (!energy_part) {
+            int64_t g = (mk.nel + 127) / 128;
+            const int64_t cap = 16 * (int64_t)num_sms();
+            g = g < cap ? g : cap;
+            if (mk.dim == 3) k_apply_K_small<3><<<(int)g, 128, 0, st>>>(mk, mom, bcmask, x, y, done);
+            else k_apply_K_small<2><<<(int)g, 128, 0, st>>>(mk, mom, bcmask, x, y, done);
+            return;
+        }
+    }
     if (mk.dim == 2) {
         if (energy_part) k_apply_K<2, R, true><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
         else k_apply_K<2, R, false><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);

@@ -55,43 +55,20 @@ __device__ __forceinline__ int32_t local_node(int32_t n0, int32_t nn0, int32_t n
 // (ld.global.cg), 2 cached weak loads (ld.global.ca).  A persistent kernel that wrote x in
 // an earlier phase of the same launch must not use 0: the non-coherent path is only valid
 // for data that no thread writes during the kernel.
-template <int DIM, typename R, int kLoad = 0, bool kEnergy = true>
-__device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R* __restrict__ mom,
-                                                        const uint8_t* __restrict__ bcmask,
-                                                        const R* __restrict__ x, R* __restrict__ y, int i, int j,
-                                                        int k, int32_t e) {
+// The arithmetic and scatter of one element, given its gathered nodal values m[c][a]
+// (corner a = (dx, dy, dz) bits) and moments M; `fixed` holds bit 8q + 4dx + c for the
+// Dirichlet components of the corners of row q.  Shared by every loader of the apply.
+template <int DIM, typename R, bool kEnergy>
+__device__ __forceinline__ double element_compute_scatter(const MeshK& mk, R (&m)[DIM][1 << DIM],
+                                                          const R (&M)[n_moments<DIM>()], uint32_t fixed,
+                                                          R* __restrict__ y, int32_t n0) {
     constexpr int NS = 1 << DIM;
-    constexpr int NM = n_moments<DIM>();
-    const int64_t nnode = mk.nnode, nel = mk.nel;
-    const int32_t nn0 = mk.nn[0], nn01 = mk.nn[0] * mk.nn[1];
-    const int32_t n0 = i + nn0 * j + (DIM == 3 ? nn01 * k : 0);
-    // corner a = (dx, dy, dz) bits; the NS/2 rows (dy, dz) start at n0 + rowoff, the x+1
-    // corner is the next word of the row
     constexpr int NR = NS / 2;
+    const int64_t nnode = mk.nnode;
+    const int32_t nn0 = mk.nn[0], nn01 = mk.nn[0] * mk.nn[1];
     int32_t rowoff[NR];
 #pragma unroll
     for (int q = 0; q < NR; q++) rowoff[q] = (q & 1) * nn0 + (DIM == 3 ? ((q >> 1) & 1) * nn01 : 0);
-    uint32_t fixed = 0;  // bit 4a + c: component c of corner a has a Dirichlet condition
-#pragma unroll
-    for (int q = 0; q < NR; q++) {
-        const uint8_t* br = bcmask + n0 + rowoff[q];
-        fixed |= ((uint32_t)br[0] | ((uint32_t)br[1] << 4)) << (8 * q);
-    }
-
-    R m[DIM][NS];
-#pragma unroll
-    for (int c = 0; c < DIM; c++) {
-#pragma unroll
-        for (int q = 0; q < NR; q++) {
-            const R* xr = x + c * nnode + n0 + rowoff[q];
-            m[c][2 * q] = kLoad == 1 ? __ldcg(xr) : kLoad == 2 ? __ldca(xr) : xr[0];
-            m[c][2 * q + 1] = kLoad == 1 ? __ldcg(xr + 1) : kLoad == 2 ? __ldca(xr + 1) : xr[1];
-        }
-    }
-    R M[NM];
-    const R* Me = mom + e;
-#pragma unroll
-    for (int q = 0; q < NM; q++) M[q] = Me[q * nel];
     R kap[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; d++) kap[d] = (R)mk.kappa[d];
@@ -171,6 +148,46 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
     return energy;
 }
 
+template <int DIM, typename R, int kLoad = 0, bool kEnergy = true>
+__device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R* __restrict__ mom,
+                                                        const uint8_t* __restrict__ bcmask,
+                                                        const R* __restrict__ x, R* __restrict__ y, int i, int j,
+                                                        int k, int32_t e) {
+    constexpr int NS = 1 << DIM;
+    constexpr int NM = n_moments<DIM>();
+    const int64_t nnode = mk.nnode, nel = mk.nel;
+    const int32_t nn0 = mk.nn[0], nn01 = mk.nn[0] * mk.nn[1];
+    const int32_t n0 = i + nn0 * j + (DIM == 3 ? nn01 * k : 0);
+    // corner a = (dx, dy, dz) bits; the NS/2 rows (dy, dz) start at n0 + rowoff, the x+1
+    // corner is the next word of the row
+    constexpr int NR = NS / 2;
+    int32_t rowoff[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) rowoff[q] = (q & 1) * nn0 + (DIM == 3 ? ((q >> 1) & 1) * nn01 : 0);
+    uint32_t fixed = 0;  // bit 4a + c: component c of corner a has a Dirichlet condition
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        const uint8_t* br = bcmask + n0 + rowoff[q];
+        fixed |= ((uint32_t)br[0] | ((uint32_t)br[1] << 4)) << (8 * q);
+    }
+
+    R m[DIM][NS];
+#pragma unroll
+    for (int c = 0; c < DIM; c++) {
+#pragma unroll
+        for (int q = 0; q < NR; q++) {
+            const R* xr = x + c * nnode + n0 + rowoff[q];
+            m[c][2 * q] = kLoad == 1 ? __ldcg(xr) : kLoad == 2 ? __ldca(xr) : xr[0];
+            m[c][2 * q + 1] = kLoad == 1 ? __ldcg(xr + 1) : kLoad == 2 ? __ldca(xr + 1) : xr[1];
+        }
+    }
+    R M[NM];
+    const R* Me = mom + e;
+#pragma unroll
+    for (int q = 0; q < NM; q++) M[q] = Me[q * nel];
+    return element_compute_scatter<DIM, R, kEnergy>(mk, m, M, fixed, y, n0);
+}
+
 // Element tiles of one 256-thread block: 32 × 4 × 2 elements in 3D, 32 × 8 in 2D, x fastest
 // (a warp is one row of 32 elements: coalesced moment loads, no index divisions).
 template <int DIM>
@@ -186,11 +203,12 @@ struct ApplyTile<2> {
 
 // y += K x over the element tiles tile0, tile0 + tstride, … (blockDim.x must be 256).
 // Returns this thread's Σ x_eᵀ K_e x_e when kEnergy.
-template <int DIM, typename R, int kLoad = 0, bool kEnergy = true>
+template <int DIM, typename R, int kLoad = 0, bool kEnergy = true, int TY = ApplyTile<DIM>::Y,
+          int TZ = ApplyTile<DIM>::Z>
 __device__ __forceinline__ double apply_tiles(const MeshK& mk, const R* __restrict__ mom,
                                               const uint8_t* __restrict__ bcmask, const R* __restrict__ x,
                                               R* __restrict__ y, int64_t tile0, int64_t tstride) {
-    constexpr int TX = ApplyTile<DIM>::X, TY = ApplyTile<DIM>::Y, TZ = ApplyTile<DIM>::Z;
+    constexpr int TX = ApplyTile<DIM>::X;
     const int ntx = (mk.n[0] + TX - 1) / TX, nty = (mk.n[1] + TY - 1) / TY;
     const int ntz = DIM == 3 ? (mk.n[2] + TZ - 1) / TZ : 1;
     const int32_t ntiles = ntx * nty * ntz;
