@@ -666,6 +666,7 @@ int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* 
         apply_K<double>(H.mk, H.mom64.as<double>(), bcmask, x, r64, H.stream);
         k_defect<<<kRedBlocks, 256, 0, H.stream>>>(nd, H.nnode, bcmask, bb, H.kdiag64.as<double>(), r64,
                                                     sc.part, sc.counter + 4, sc.out + 1);
+        H.kernel_launches += 4;  // to FP32, refine step, FP64 apply, defect
         double rn;
         GG_CUDA(cudaMemcpyAsync(&rn, sc.out + 1, sizeof(double), cudaMemcpyDeviceToHost, H.stream));
         GG_CUDA(cudaStreamSynchronize(H.stream));
@@ -770,15 +771,18 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     // STEP 1 (:553-565)
     if ((rc = inner(f, vstar, prm.tolerance)) != GG_OK) return fail("first inner solve (K u* = f)", rc);
     apply_GT(H, vstar, qtmp, st);
+    H.kernel_launches++;
     axpby(H, ne, -1.0, hv, 1.0, qtmp);
     const double inner_rtol = prm.inner_rtol_factor * prm.tolerance;
     const double rhs_scale = sqrt(dot(H, ne, qtmp, qtmp)) / scaleq;
     if (!isfinite(rhs_scale)) return GG_ERR_NONFINITE;
     // STEP 3 (:616-659)
     apply_G(H, q, ftmp, st);
+    H.kernel_launches++;
     axpby(H, nd, 1.0, f, -1.0, ftmp);
     if ((rc = inner(ftmp, u, inner_rtol)) != GG_OK) return fail("velocity solve K u = f - G p", rc);
     apply_GT(H, u, r, st);
+    H.kernel_launches++;
     axpby(H, ne, -1.0, hv, 1.0, r);
     // STEP 4 (:664-837)
     double zr_prev = 1.0, absres = 0.0, relres = 0.0;
@@ -795,6 +799,7 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
         else
             axpby(H, ne, 1.0, qtmp, zr / zr_prev, s);
         apply_G(H, s, ftmp, st);
+        H.kernel_launches++;
         // recycling (fast path only): s = z + β s_prev, so β u*_prev = K⁻¹ G (β s_prev)
         // is a start for K u* = G s that leaves only K⁻¹ G z to find; the stopping rule
         // stays relative to ‖G s‖
@@ -802,6 +807,7 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
         if (warm) axpby(H, nd, 0.0, vstar, zr / zr_prev, vstar);
         if ((rc = inner(ftmp, vstar, inner_rtol, warm)) != GG_OK) return fail("inner solve K u* = G s", rc);
         apply_GT(H, vstar, qtmp, st);
+        H.kernel_launches++;
         const double sq = dot(H, ne, s, qtmp);
         const double alpha = zr / sq;
         if (!isfinite(zr) || !isfinite(sq) || !isfinite(alpha)) return fail("conjugate-direction step", GG_ERR_NONFINITE);
