@@ -20,16 +20,21 @@ struct KrylovScalars {
     int32_t done, iterations, failed, maxit;
 };
 
+// Device memory of the handle buffers (gg_alloc.cu): pooled up to 4 MB, cudaMalloc above.
+void* dev_alloc(size_t bytes, int* dev_out);
+void dev_free(void* p, size_t bytes, int dev);
+
 // A device buffer with RAII.
 struct DBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    int dev = -1;
     DBuf() = default;
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
     ~DBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p, bytes, dev);
         p = nullptr;
         bytes = 0;
     }
@@ -37,7 +42,7 @@ struct DBuf {
         if (nbytes <= bytes && p) return;
         release();
         size_t b = nbytes ? nbytes : 16;
-        GG_CUDA(cudaMalloc(&p, b));
+        p = dev_alloc(b, &dev);
         bytes = b;
     }
     template <class T>
