@@ -19,11 +19,14 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
+#include "gg_grid.cuh"
 #include "gg_ops.cuh"
 
 namespace gg {
@@ -330,14 +333,30 @@ __global__ void k_power_step(int64_t n, const float* __restrict__ invd, const fl
     }
 }
 
-__global__ void k_scale(int64_t n, float s, const float* __restrict__ y, float* __restrict__ x) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        x[i] = s * y[i];
+// Σ of the nb block partials in block order (one thread): state[0] = λ = √(‖y‖²/‖x‖²),
+// state[1] = 1/‖y‖, state[2] ≠ 0 once a step was degenerate (λ then keeps its last value
+// and x is no longer rescaled).
+__global__ void k_power_norm(int nb, const double* __restrict__ part, double* __restrict__ state) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double yy = 0, xx = 0;
+    for (int b = 0; b < nb; b++) {
+        yy += part[2 * b];
+        xx += part[2 * b + 1];
+    }
+    if (state[2] != 0.0 || xx <= 0 || yy <= 0) {
+        state[2] = 1.0;
+        return;
+    }
+    state[0] = sqrt(yy / xx);
+    state[1] = 1.0 / sqrt(yy);
 }
 
-__global__ void k_unit(int64_t n, int64_t j, double* __restrict__ x) {
+__global__ void k_scale(int64_t n, const double* __restrict__ state, const float* __restrict__ y,
+                        float* __restrict__ x) {
+    if (state[2] != 0.0) return;
+    const float s = (float)state[1];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        x[i] = (i == j) ? 1.0 : 0.0;
+        x[i] = s * y[i];
 }
 
 int g(int64_t n) { return grid_for(n, 256); }
@@ -436,25 +455,26 @@ static double power_lambda(Handle& H, MGLevel& L) {
     cudaStream_t st = H.stream;
     const int64_t n = L.ndof;
     const int nb = 64;
-    H.mg_part.ensure(sizeof(double) * 2 * nb);
-    std::vector<double> part(2 * nb);
+    H.mg_part.ensure(sizeof(double) * (2 * nb + 4));
+    double* part = H.mg_part.as<double>();
+    double* state = part + 2 * nb;
     float* x = L.x.as<float>();
     float* y = L.d.as<float>();
     float* t = L.t.as<float>();
     k_hash_fill<<<g(n), 256, 0, st>>>(n, L.nnode, L.bcmask, x);
     GG_CUDA(cudaMemsetAsync(t, 0, sizeof(float) * n, st));
-    double lam = 0.0;
+    GG_CUDA(cudaMemsetAsync(state, 0, sizeof(double) * 4, st));
+    // 12 steps queued without a host round trip; λ is read once at the end
     for (int it = 0; it < 12; it++) {
         apply_K_ex<float>(L.mk, L.mom32, L.bcmask, x, t, nullptr, apply_grid(L.nel), st, nullptr);
-        k_power_step<<<nb, 256, 0, st>>>(n, L.invdiag.as<float>(), x, t, y, H.mg_part.as<double>());
-        GG_CUDA(cudaMemcpyAsync(part.data(), H.mg_part.p, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, st));
-        GG_CUDA(cudaStreamSynchronize(st));
-        double yy = 0, xx = 0;
-        for (int b = 0; b < nb; b++) { yy += part[2 * b]; xx += part[2 * b + 1]; }
-        if (xx <= 0 || yy <= 0) break;
-        lam = sqrt(yy / xx);
-        k_scale<<<g(n), 256, 0, st>>>(n, (float)(1.0 / sqrt(yy)), y, x);
+        k_power_step<<<nb, 256, 0, st>>>(n, L.invdiag.as<float>(), x, t, y, part);
+        k_power_norm<<<1, 32, 0, st>>>(nb, part, state);
+        k_scale<<<g(n), 256, 0, st>>>(n, state, y, x);
     }
+    H.kernel_launches += 2 + 4 * 12;
+    double lam = 0.0;
+    GG_CUDA(cudaMemcpyAsync(&lam, state, sizeof(double), cudaMemcpyDeviceToHost, st));
+    GG_CUDA(cudaStreamSynchronize(st));
     GG_CUDA(cudaGetLastError());
     return lam;
 }
@@ -493,6 +513,30 @@ __global__ void k_gj_step(int64_t n, int64_t c, const double* __restrict__ in, d
     }
 }
 
+// All n Gauss–Jordan steps in one cooperative launch: step c reads `in` and writes `out` as
+// k_gj_step does, then the grid meets at a barrier and the buffers swap.  `in` was written
+// by other blocks in this launch, so it is read through L2 (ld.global.cg).  A barrier that
+// gives up (error word in gb) ends every block; the host reports it.
+__global__ void k_gj_all(int64_t n, double* __restrict__ m0, double* __restrict__ m1, GridBarrier* gb) {
+    unsigned int epoch = 0;
+    const int64_t w = 2 * n;
+    double* in = m0;
+    double* out = m1;
+    for (int64_t c = 0; c < n; c++) {
+        const double inv_p = 1.0 / __ldcg(&in[c * w + c]);
+        for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * w;
+             q += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t i = q / w, k = q - i * w;
+            const double pk = __ldcg(&in[c * w + k]) * inv_p;
+            out[q] = i == c ? pk : __ldcg(&in[q]) - __ldcg(&in[i * w + c]) * pk;
+        }
+        if (!grid_barrier(gb, &epoch)) return;
+        double* t = in;
+        in = out;
+        out = t;
+    }
+}
+
 __global__ void k_gj_extract(int64_t n, const double* __restrict__ M, float* __restrict__ inv) {
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * n; q += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = q / n, k = q - i * n;
@@ -502,6 +546,44 @@ __global__ void k_gj_extract(int64_t n, const double* __restrict__ M, float* __r
 
 // Dense FP32 inverse of the coarsest operator: its columns by unit-vector applies, then
 // Gauss–Jordan on the device (n steps of one kernel each).
+// Column j of the coarsest operator, A[:, j] = K e_j, from every element that touches dof
+// j: one thread per (element, element-local dof), the element arithmetic of the apply on
+// the unit vector, scattered into column j (BC rows skipped; columns of BC dofs stay zero).
+template <int DIM>
+__global__ void k_coarse_columns(MeshK mk, const double* __restrict__ mom, const uint8_t* __restrict__ bc,
+                                 double* __restrict__ A) {
+    constexpr int NS = 1 << DIM, NR = NS / 2, NM = n_moments<DIM>();
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < mk.nel * NS * DIM;
+         q += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t e = (int32_t)(q / (NS * DIM));
+    const int loc = (int)(q - (int64_t)e * NS * DIM);
+    const int ja = loc / DIM, jc = loc - ja * DIM;  // corner and component of the column's dof
+    int ijk[3];
+    elem_ijk(mk, e, ijk);
+    const int32_t nn0 = mk.nn[0], nn01 = mk.nn[0] * mk.nn[1];
+    const int32_t n0 = ijk[0] + nn0 * ijk[1] + (DIM == 3 ? nn01 * ijk[2] : 0);
+    uint32_t fixed = 0;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const uint8_t* br = bc + n0 + (r & 1) * nn0 + (DIM == 3 ? ((r >> 1) & 1) * nn01 : 0);
+        fixed |= ((uint32_t)br[0] | ((uint32_t)br[1] << 4)) << (8 * r);
+    }
+    // corner ja = (dx, dy, dz) sits in row ja >> 1 at word dx
+    if ((fixed >> (8 * (ja >> 1) + 4 * (ja & 1) + jc)) & 1) continue;
+    const int32_t node = n0 + (ja & 1) + ((ja >> 1) & 1) * nn0 + (DIM == 3 ? ((ja >> 2) & 1) * nn01 : 0);
+    double m[DIM][NS];
+#pragma unroll
+    for (int c = 0; c < DIM; c++)
+#pragma unroll
+        for (int a = 0; a < NS; a++) m[c][a] = (c == jc && a == ja) ? 1.0 : 0.0;
+    double M[NM];
+#pragma unroll
+    for (int k = 0; k < NM; k++) M[k] = mom[(int64_t)k * mk.nel + e];
+    double* col = A + ((int64_t)jc * mk.nnode + node) * ((int64_t)DIM * mk.nnode);
+    element_compute_scatter<DIM, double, false>(mk, m, M, fixed, col, n0);
+    }
+}
+
 static void coarse_inverse(Handle& H, MGLevel& L) {
     const int64_t n = L.ndof;
     cudaStream_t st = H.stream;
@@ -510,22 +592,48 @@ static void coarse_inverse(Handle& H, MGLevel& L) {
     double* e = A + n * n;
     double* M0 = e + n;
     double* M1 = M0 + 2 * n * n;
+    (void)e;
     GG_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * n * n, st));
-    std::vector<uint8_t> bc(L.nnode);
-    GG_CUDA(cudaMemcpyAsync(bc.data(), L.bcmask, L.nnode, cudaMemcpyDeviceToHost, st));
-    GG_CUDA(cudaStreamSynchronize(st));
-    auto fixed = [&](int64_t i) { const int c = (int)(i / L.nnode); return (bc[i - c * L.nnode] >> c) & 1; };
-    for (int64_t j = 0; j < n; j++) {
-        if (fixed(j)) continue;
-        k_unit<<<g(n), 256, 0, st>>>(n, j, e);
-        apply_K_ex<double>(L.mk, L.mom64, L.bcmask, e, A + j * n, nullptr, apply_grid(L.nel), st, nullptr);
-        H.kernel_launches += 2;
-    }
+    const int64_t threads = L.nel * (int64_t)(H.dim == 3 ? 24 : 8);
+    if (H.dim == 3) k_coarse_columns<3><<<grid_for(threads, 128), 128, 0, st>>>(L.mk, L.mom64, L.bcmask, A);
+    else k_coarse_columns<2><<<grid_for(threads, 128), 128, 0, st>>>(L.mk, L.mom64, L.bcmask, A);
+    H.kernel_launches++;
     const int gb = grid_for(2 * n * n, 256);
     k_gj_init<<<gb, 256, 0, st>>>(n, L.nnode, L.bcmask, A, M0);
-    for (int64_t c = 0; c < n; c++) {
-        k_gj_step<<<gb, 256, 0, st>>>(n, c, M0, M1);
-        std::swap(M0, M1);
+    // one cooperative launch with a grid barrier between steps where the device allows it
+    // (n barriers of ~2 µs instead of n launches); else one launch per step
+    static std::atomic<int> coop_blocks[64];  // co-resident blocks of k_gj_all per device (0: not probed)
+    int dev = 0;
+    GG_CUDA(cudaGetDevice(&dev));
+    int coop = 0;
+    if (dev >= 0 && dev < 64) {
+        if (coop_blocks[dev].load() == 0) {
+            int attr = 0, per_sm = 0;
+            GG_CUDA(cudaDeviceGetAttribute(&attr, cudaDevAttrCooperativeLaunch, dev));
+            if (attr) GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_all, 256, 0));
+            coop_blocks[dev].store(attr && per_sm > 0 ? per_sm * num_sms() : -1);
+        }
+        coop = coop_blocks[dev].load();
+    }
+    if (coop > 0) {
+        const int grid = std::min(coop, gb);
+        H.fused_bar.ensure(sizeof(GridBarrier));
+        GridBarrier* bar = H.fused_bar.as<GridBarrier>();
+        GG_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), st));
+        int64_t nn = n;
+        void* args[] = {(void*)&nn, (void*)&M0, (void*)&M1, (void*)&bar};
+        GG_CUDA(cudaLaunchCooperativeKernel((const void*)k_gj_all, dim3(grid), dim3(256), args, 0, st));
+        GridBarrier hb{};
+        GG_CUDA(cudaMemcpyAsync(&hb, bar, sizeof(GridBarrier), cudaMemcpyDeviceToHost, st));
+        GG_CUDA(cudaStreamSynchronize(st));
+        if (hb.err) throw CudaError(cudaErrorLaunchTimeout, "k_gj_all grid barrier gave up", __FILE__, __LINE__);
+        if (n & 1) std::swap(M0, M1);  // the last step wrote the other buffer
+        H.kernel_launches += 1 - n;    // one launch instead of n (counted below)
+    } else {
+        for (int64_t c = 0; c < n; c++) {
+            k_gj_step<<<gb, 256, 0, st>>>(n, c, M0, M1);
+            std::swap(M0, M1);
+        }
     }
     H.coarse_inv.ensure(sizeof(float) * n * n);
     k_gj_extract<<<grid_for(n * n, 256), 256, 0, st>>>(n, M0, H.coarse_inv.as<float>());
