@@ -22,11 +22,15 @@ void store_solution(Handle& H);
 namespace {
 
 int solve_one(gg_handle* h, const gg_uzawa_params* prm, double* u, double* p, gg_uzawa_stats* st) {
+    // share the GPU with the other problems of the batch; a later lone solve gets the
+    // handle's own setting back
+    const int keep = h->H.fused_dofs_per_block;
+    h->H.fused_dofs_per_block = 1024;
     int rc = gg_locate(h, nullptr);
-    if (rc != GG_OK) return rc;
-    rc = gg_build_operator(h, prm->precision, 0, nullptr, nullptr);
-    if (rc != GG_OK) return rc;
-    return gg_uzawa_solve(h, prm, u, p, st);
+    if (rc == GG_OK) rc = gg_build_operator(h, prm->precision, 0, nullptr, nullptr);
+    if (rc == GG_OK) rc = gg_uzawa_solve(h, prm, u, p, st);
+    h->H.fused_dofs_per_block = keep;
+    return rc;
 }
 
 }  // namespace

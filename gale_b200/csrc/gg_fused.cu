@@ -551,7 +551,8 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
         H.fused_phases = T.nphase;
     }
     const int64_t n = H.ndof;
-    int grid = (int)std::min<int64_t>((int64_t)max_blocks, (n + kFusedBlock - 1) / kFusedBlock);
+    const int64_t per = H.fused_dofs_per_block > 0 ? H.fused_dofs_per_block : kFusedBlock;
+    int grid = (int)std::min<int64_t>((int64_t)max_blocks, (n + per - 1) / per);
     if (grid < 1) grid = 1;
     // the barrier counter reaches (barriers of the launch) × grid: keep it inside 32 bits
     if ((double)(maxit + 2) * (H.fused_phases + 1) * grid >= 2147483648.0) return 1;

@@ -121,6 +121,10 @@ struct Handle {
     const float* fused_r = nullptr;  // FCG residual / preconditioned vector baked into it
     const float* fused_z = nullptr;
     int fused_phases = 0;            // grid barriers per iteration
+    // dofs per block of the persistent kernel's grid: 256 for a problem solved alone; 1024
+    // when gg_solve_batch runs it beside others (fewer blocks per problem, more problems
+    // resident at once: 512 sinkers 94 -> 107 solves/s, a lone 256x64 problem 10 % slower)
+    int fused_dofs_per_block = 256;
     // learned coarse correction (gg_learned.cu)
     std::shared_ptr<struct LearnedState> learned;
     bool nn_ready = false;
