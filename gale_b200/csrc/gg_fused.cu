@@ -503,7 +503,7 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
             F.r = L.r.as<float>();
             F.d = L.d.as<float>();
             F.t = L.t.as<float>();
-            const ChebCoef cc = cheb_coef(L.lambda_max, deg);
+            const ChebCoef cc = cheb_coef(L.lambda_max, level_degree(H, l));
             F.inv_theta = cc.inv_theta;
             for (int k = 0; k < 4; k++) {
                 F.c1[k] = cc.c1[k];
@@ -518,7 +518,8 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
         };
         const int ns = (int)nl - 1;  // smoothed levels
         for (int l = 0; l < ns; l++) {
-            for (int k = 1; k < deg; k++) {
+            const int dl = level_degree(H, l);
+            for (int k = 1; k < dl; k++) {
                 ph(PH_APPLY, l, 0, 0);
                 ph(PH_STEP, l, k);
             }
@@ -530,9 +531,10 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
             ph(PH_PROLONG, l);
             ph(PH_APPLY, l, 0, 1);
             ph(PH_RESTART, l);
-            for (int k = 1; k < deg; k++) {
+            const int dl = level_degree(H, l);
+            for (int k = 1; k < dl; k++) {
                 ph(PH_APPLY, l, 0, 0);
-                ph(l == 0 && k == deg - 1 ? PH_STEP_DOTS : PH_STEP, l, k);
+                ph(l == 0 && k == dl - 1 ? PH_STEP_DOTS : PH_STEP, l, k);
             }
         }
         ph(PH_DIR, 0);

@@ -72,6 +72,8 @@ struct ChebCoef {
     float c1[8], c2[8];
 };
 ChebCoef cheb_coef(double lmax_est, int degree);
+// Chebyshev degree of level l's smoother (the configured degree on the fine level)
+int level_degree(const Handle& H, size_t l);
 int mg_setup(Handle& H);
 void vcycle(Handle& H, size_t l, const float* b, float* x, const int32_t* done);
 void mg_restrict(Handle& H, size_t l, const float* fine, float* coarse, const int32_t* done);

@@ -174,7 +174,8 @@ def UzawaSolver(tolerance=1e-5, maxIterations=1000, minIterations=1,
                 reusePressure=False, recycle=None, smoothingDegree=0) -> abi.UzawaParams:
     """Stokes_SLE_UzawaSolver XML parameters (Stokes_SLE_UzawaSolver.cxx:241-264).
     recycle (default: on for the mixed path) starts each inner solve from β u*_prev;
-    smoothingDegree (2..4, 0 = 2) is the multigrid Chebyshev degree per level and sweep."""
+    smoothingDegree (2..4, 0 = 2) is the multigrid Chebyshev degree of each fine-level sweep;
+    coarser levels use min(smoothingDegree, 2)."""
     p = abi.UzawaParams()
     p.tolerance = tolerance
     p.max_iterations = maxIterations

@@ -153,7 +153,8 @@ typedef struct gg_uzawa_params {
                                      K u* = G s from β u*_prev (s = z + β s_prev); the
                                      inner stopping rule stays relative to ‖G s‖        */
     int32_t smoothing_degree;     /* multigrid: Chebyshev degree of the pre- and post-
-                                     smoothing on every level, 2..4 (0: 2); the role of
+                                     smoothing on the fine level, 2..4 (0: 2); coarser
+                                     levels use min(degree, 2); the role of
                                      PETScMGSolver's downIterations/upIterations
                                      (PETScMGSolver.cxx:182-183)                         */
 } gg_uzawa_params;
