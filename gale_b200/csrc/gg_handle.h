@@ -125,6 +125,9 @@ struct Handle {
     // when gg_solve_batch runs it beside others (fewer blocks per problem, more problems
     // resident at once: 512 sinkers 94 -> 107 solves/s, a lone 256x64 problem 10 % slower)
     int fused_dofs_per_block = 256;
+    // the multigrid refinement sweeps of this Uzawa solve aim at 1e-5 instead of 1e-4 once an
+    // inner solve has needed more than two sweeps (set in inner_solve, reset per Uzawa solve)
+    bool tight_sweeps = false;
     // learned coarse correction (gg_learned.cu)
     std::shared_ptr<struct LearnedState> learned;
     bool nn_ready = false;
