@@ -481,7 +481,7 @@ static double power_lambda(Handle& H, MGLevel& L) {
         k_power_norm<<<1, 32, 0, st>>>(nb, part, state);
         k_scale<<<g(n), 256, 0, st>>>(n, state, y, x);
     }
-    H.kernel_launches += 2 + 4 * 12;
+    H.kernel_launches += 1 + 4 * 12;  // start vector, then 12 × (apply, step, norm, scale)
     double lam = 0.0;
     GG_CUDA(cudaMemcpyAsync(&lam, state, sizeof(double), cudaMemcpyDeviceToHost, st));
     GG_CUDA(cudaStreamSynchronize(st));
@@ -716,8 +716,9 @@ int mg_setup(Handle& H) {
         GG_CUDA(cudaGetLastError());
     }
     for (auto& L : H.mg) L->lambda_max = power_lambda(H, *L);
-    // diag inversion + per coarse level (mask, moments, diag, inversion) + power iterations
-    H.kernel_launches += 1 + 4 * (int64_t)(H.mg.size() - 1) + 37 * (int64_t)H.mg.size();
+    // diag inversion + per coarse level (mask, moments, diag, inversion); power_lambda counts
+    // its own launches
+    H.kernel_launches += 1 + 4 * (int64_t)(H.mg.size() - 1);
     MGLevel& Lc = *H.mg.back();
     H.coarse_n = 0;
     if (H.mg.size() > 1 && Lc.ndof <= 3000) coarse_inverse(H, Lc);
