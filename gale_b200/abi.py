@@ -68,6 +68,10 @@ class Rheology(C.Structure):
         ("minimum_yield_stress", C.c_double), ("minimum_viscosity", C.c_double),
         ("max_strain_rate", C.c_double), ("depth_coefficient", C.c_double),
         ("strain_rate_softening", C.c_int32), ("pad", C.c_int32),
+        ("boundary_cohesion", C.c_double), ("boundary_cohesion_after_softening", C.c_double),
+        ("boundary_friction_coefficient", C.c_double),
+        ("boundary_friction_coefficient_after_softening", C.c_double),
+        ("boundary_walls", C.c_int32), ("hydrostatic_term", C.c_int32),
     ]
 
 

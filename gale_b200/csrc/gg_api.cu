@@ -275,9 +275,15 @@ int gg_set_velocity_bc_nodes(gg_handle* h, const uint8_t* fixed, const double* v
 
 int gg_set_materials(gg_handle* h, int32_t n, const gg_material* mats) {
     if (!h || !mats || n < 1 || n > GG_MAX_MATERIALS) return h ? gg::set_error(h->H, GG_ERR_INVALID, "material count") : GG_ERR_INVALID;
-    for (int i = 0; i < n; i++)
+    for (int i = 0; i < n; i++) {
         if (mats[i].n_rheologies < 0 || mats[i].n_rheologies > GG_MAX_RHEOLOGIES)
             return gg::set_error(h->H, GG_ERR_INVALID, "rheology count");
+        // DruckerPrager's HydrostaticTerm (DruckerPrager.cxx:327-332) adds a lithostatic
+        // pressure this library does not evaluate: refused rather than silently dropped
+        for (int k = 0; k < mats[i].n_rheologies; k++)
+            if (mats[i].rheology[k].hydrostatic_term)
+                return gg::set_error(h->H, GG_ERR_INVALID, "DruckerPrager HydrostaticTerm is not supported");
+    }
     h->H.materials.assign(mats, mats + n);
     h->H.n_materials = n;
     h->H.built = false;

@@ -312,10 +312,7 @@ int gg_learned_train(gg_handle* h, const gg_learn_params* params, gg_learn_stats
             b->ensure(sizeof(float) * H.ndof);
         H.qtmp.ensure(sizeof(double) * H.nel);
         H.ftmp.ensure(sizeof(double) * H.ndof);
-        H.red.ensure(sizeof(double) * (4 * 592 + 8) + sizeof(unsigned int) * 8);
-        GG_CUDA(cudaMemsetAsync(reinterpret_cast<double*>(H.red.p) + 4 * 592 + 8, 0, sizeof(unsigned int) * 8, H.stream));
-        H.scal.ensure(sizeof(gg::KrylovScalars) * 2);
-        if (!H.h_scal) GG_CUDA(cudaMallocHost(&H.h_scal, sizeof(gg::KrylovScalars) * 2));
+        gg::prepare_krylov_scratch(H);
         rc = gg::learned_train(H, *params, S);
     })
     if (stats) *stats = S;

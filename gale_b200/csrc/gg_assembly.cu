@@ -19,7 +19,9 @@
 // Kernel shape: a CTA owns 128 consecutive elements and walks their contiguous point
 // range in chunks of 512.  Phase 1 (one thread per point, coalesced loads): rheology,
 // c_p, force weights → shared memory.  Phase 2 (one thread per element): sequential
-// sums in point order, i.e. the reference's summation order.
+// sums in point order, i.e. the reference's summation order.  The element's corner terms
+// of the K diagonal and of the force go to per-element buffers; k_gather_corners sums
+// them per node in a fixed element order, so a build gives the same bits on every run.
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -166,9 +168,17 @@ __device__ PointOut run_rheologies(const MeshK& mk, const gg_material& m, const 
                 crit = (R)r.cohesion * (R(1) - ratio) + (R)r.cohesion_after_softening * ratio;
             } else if (kind == GG_RHEO_DRUCKER_PRAGER) {  // DruckerPrager.cxx:296-412
                 const R pressure = pp ? (R)pp[e] : R(0);
-                const R mu = (R)r.friction_coefficient * (R(1) - ratio) +
-                             (R)r.friction_coefficient_after_softening * ratio;
-                const R C = (R)r.cohesion * (R(1) - ratio) + (R)r.cohesion_after_softening * ratio;
+                // elements along a flagged wall take the boundary strength (:341-361)
+                const int bw = r.boundary_walls;
+                const bool inb = ((bw & 1) && ijk[0] == 0) || ((bw & 2) && ijk[0] == mk.n[0] - 1) ||
+                                 ((bw & 4) && ijk[1] == 0) || ((bw & 8) && ijk[1] == mk.n[1] - 1) ||
+                                 (DIM == 3 && (((bw & 16) && ijk[2] == 0) || ((bw & 32) && ijk[2] == mk.n[2] - 1)));
+                const R mu = inb ? (R)r.boundary_friction_coefficient * (R(1) - ratio) +
+                                       (R)r.boundary_friction_coefficient_after_softening * ratio
+                                 : (R)r.friction_coefficient * (R(1) - ratio) +
+                                       (R)r.friction_coefficient_after_softening * ratio;
+                const R C = inb ? (R)r.boundary_cohesion * (R(1) - ratio) + (R)r.boundary_cohesion_after_softening * ratio
+                                : (R)r.cohesion * (R(1) - ratio) + (R)r.cohesion_after_softening * ratio;
                 R factor, fs;
                 if (DIM == 2) {
                     factor = R(1) / r_sqrt<R>(R(1) + mu * mu);
@@ -222,8 +232,8 @@ k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
                 const double* __restrict__ ps_s, const double* __restrict__ T,
                 const double* __restrict__ pu, const double* __restrict__ pp, int prev,
                 double gravity, double g0, double g1, double g2, double rayleigh, int want_force,
-                R* __restrict__ mom, R* __restrict__ kdiag, double* __restrict__ sdiag,
-                double* __restrict__ f, double* __restrict__ eta_s, double* __restrict__ incr_s,
+                R* __restrict__ mom, R* __restrict__ kcorner, double* __restrict__ sdiag,
+                double* __restrict__ fcorner, double* __restrict__ eta_s, double* __restrict__ incr_s,
                 uint8_t* __restrict__ yld_s, int32_t* __restrict__ flag,
                 const gg_material* __restrict__ materials, const double* __restrict__ w_s) {
     constexpr int NM = n_moments<DIM>();
@@ -369,22 +379,61 @@ k_build_moments(MeshK mk, int64_t nel, const int32_t* __restrict__ offsets,
         double tot = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; d++) tot += S[d];
-        const int64_t n = elem_node<DIM>(mk, ijk, a);
 #pragma unroll
         for (int c = 0; c < DIM; c++) {
             const double dg = tot + S[c];
-            atomicAdd(&kdiag[(int64_t)c * mk.nnode + n], (R)dg);
+            kcorner[(int64_t)(a * DIM + c) * nel + e] = (R)dg;
             // Ĝ_e = Σ G_e² / K_e diagonal, over every dof (UzawaPreconditionerTerm.cxx:199-215)
             sd += mk.Ge[a][c] * (mk.Ge[a][c] / dg);
-            if (want_force) {
-                const double gc = c == 0 ? g0 : (c == 1 ? g1 : g2);
-                double fv = gc * F[a];
-                if (c == 1) fv += Psi[a];
-                atomicAdd(&f[(int64_t)c * mk.nnode + n], fv);
-            }
+        }
+        if (want_force) {
+            fcorner[(int64_t)a * nel + e] = F[a];
+            fcorner[(int64_t)(NEN + a) * nel + e] = Psi[a];
         }
     }
     if (sdiag) sdiag[e] = sd;
+}
+
+// Node sums of the element corner terms in a fixed element order (corner a' = 0 … 2^dim−1
+// of the node in its adjacent elements), so the assembled diagonal and force vector are
+// the same bits on every run: kdiag[c][n] = Σ_e K_e[(a',c),(a',c)],
+// f[c][n] = Σ_e (g_c F_e[a'] + [c = y] Ψ_e[a']).
+template <int DIM, typename R>
+__global__ void k_gather_corners(MeshK mk, const R* __restrict__ kcorner, const double* __restrict__ fcorner,
+                                 double g0, double g1, double g2, R* __restrict__ kdiag, double* __restrict__ f) {
+    constexpr int NEN = 1 << DIM;
+    const int64_t nnode = mk.nnode, nel = mk.nel;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nnode; n += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(n % mk.nn[0]);
+        const int j = (int)((n / mk.nn[0]) % mk.nn[1]);
+        const int k = DIM == 3 ? (int)(n / ((int64_t)mk.nn[0] * mk.nn[1])) : 0;
+        R kd[DIM];
+        double fv[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) { kd[c] = R(0); fv[c] = 0.0; }
+#pragma unroll
+        for (int a = 0; a < NEN; a++) {
+            const int ei = i - (a & 1), ej = j - ((a >> 1) & 1), ek = DIM == 3 ? k - ((a >> 2) & 1) : 0;
+            if (ei < 0 || ej < 0 || ek < 0 || ei >= mk.n[0] || ej >= mk.n[1] || (DIM == 3 && ek >= mk.n[2])) continue;
+            const int64_t e = ei + (int64_t)mk.n[0] * (ej + (int64_t)mk.n[1] * ek);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) kd[c] += kcorner[(int64_t)(a * DIM + c) * nel + e];
+            if (f) {
+                const double Fa = fcorner[(int64_t)a * nel + e], Pa = fcorner[(int64_t)(NEN + a) * nel + e];
+#pragma unroll
+                for (int c = 0; c < DIM; c++) {
+                    double v = (c == 0 ? g0 : (c == 1 ? g1 : g2)) * Fa;
+                    if (c == 1) v += Pa;
+                    fv[c] += v;
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < DIM; c++) {
+            kdiag[(int64_t)c * nnode + n] = kd[c];
+            if (f) f[(int64_t)c * nnode + n] = fv[c];
+        }
+    }
 }
 
 }  // namespace
@@ -408,9 +457,20 @@ static void launch_shape(Handle& H, int prev, const double* pu, const double* pp
     k_build_moments<DIM, R, EPC, CH><<<grid, EPC, 0, H.stream>>>(
         H.mk, nel, H.offsets.as<int32_t>(), H.xi_s.as<double>(), H.np_in, H.mat_s.as<int32_t>(),
         H.ps_s.as<double>(), T, pu, pp, prev, H.force.gravity, g[0], g[1], g[2], H.force.rayleigh,
-        f ? 1 : 0, mom, kdiag, sdiag, f, outputs ? H.eta_s.as<double>() : nullptr,
+        f ? 1 : 0, mom, reinterpret_cast<R*>(H.kcorner.p), sdiag, f ? H.fcorner.as<double>() : nullptr,
+        outputs ? H.eta_s.as<double>() : nullptr,
         H.incr_s.as<double>(), H.yld_s.as<uint8_t>(), H.flag.as<int32_t>(), H.d_materials.as<gg_material>(),
         H.weights.mode == GG_WEIGHTS_DVC && H.dvc_valid ? H.w_s.as<double>() : nullptr);
+    GG_CUDA(cudaGetLastError());
+}
+
+// kdiag (and f) from the corner terms of the last build launch
+template <int DIM, typename R>
+static void gather_corners(Handle& H, R* kdiag, double* f) {
+    double g[3] = {H.force.g_hat[0], H.force.g_hat[1], H.force.g_hat[2]};
+    const double* fc = f ? H.fcorner.as<double>() : nullptr;
+    k_gather_corners<DIM, R><<<grid_for(H.nnode, 256), 256, 0, H.stream>>>(
+        H.mk, reinterpret_cast<const R*>(H.kcorner.p), fc, g[0], g[1], g[2], kdiag, f);
     GG_CUDA(cudaGetLastError());
 }
 
@@ -426,8 +486,8 @@ static void launch_build_shape(int shape, Handle& H, int prev, const double* pu,
 }
 
 // Autotuner: the first build of a (device, dim, precision, points-per-element class) times
-// every CTA shape once on the real inputs (the atomically accumulated outputs are cleared
-// before each trial) and keeps the fastest for the rest of the process.
+// every CTA shape once on the real inputs (each trial overwrites every output) and keeps
+// the fastest for the rest of the process.
 struct BuildTuner {
     std::mutex mu;
     std::map<std::tuple<int, int, int, int>, int> best;
@@ -451,16 +511,10 @@ static void launch_build(Handle& H, int prev, const double* pu, const double* pp
         auto it = tuner().best.find(key);
         if (it != tuner().best.end()) shape = it->second;
     }
-    const int64_t nd = H.ndof;
-    auto clear = [&]() {
-        GG_CUDA(cudaMemsetAsync(kdiag, 0, sizeof(R) * nd, H.stream));
-        if (f) GG_CUDA(cudaMemsetAsync(f, 0, sizeof(double) * nd, H.stream));
-    };
     if (shape < 0) {
         float best_ms = 1e30f;
         int best = 2;
         for (int k = 0; k < kNumShapes; k++) {
-            clear();
             GG_CUDA(cudaEventRecord(H.ev0, H.stream));
             launch_build_shape<DIM, R>(k, H, prev, pu, pp, mom, kdiag, sdiag, f, outputs);
             GG_CUDA(cudaEventRecord(H.ev1, H.stream));
@@ -475,10 +529,10 @@ static void launch_build(Handle& H, int prev, const double* pu, const double* pp
         shape = best;
         std::lock_guard<std::mutex> lk(tuner().mu);
         tuner().best[key] = shape;
-        clear();
     }
     H.build_shape[sizeof(R) == 4 ? 1 : 0] = shape;
     launch_build_shape<DIM, R>(shape, H, prev, pu, pp, mom, kdiag, sdiag, f, outputs);
+    gather_corners<DIM, R>(H, kdiag, f);
 }
 
 int build_operator(Handle& H, int precision, int prev, const double* d_prev_u,
@@ -491,9 +545,11 @@ int build_operator(Handle& H, int precision, int prev, const double* d_prev_u,
     H.sdiag.ensure(sizeof(double) * nel);
     H.f.ensure(sizeof(double) * nd);
     H.flag.ensure(sizeof(int32_t) * 4);
+    // element corner terms of the diagonal and the force, summed per node after the build
+    const int nen = 1 << H.dim;
+    H.kcorner.ensure(sizeof(double) * nen * H.dim * nel);
+    H.fcorner.ensure(sizeof(double) * 2 * nen * nel);
     upload_materials(H);
-    GG_CUDA(cudaMemsetAsync(H.kdiag64.p, 0, sizeof(double) * nd, st));
-    GG_CUDA(cudaMemsetAsync(H.f.p, 0, sizeof(double) * nd, st));
     GG_CUDA(cudaMemsetAsync(H.flag.p, 0, sizeof(int32_t) * 4, st));
     if (H.dim == 2)
         launch_build<2, double>(H, prev, d_prev_u, d_prev_p, H.mom64.as<double>(), H.kdiag64.as<double>(),
@@ -504,7 +560,6 @@ int build_operator(Handle& H, int precision, int prev, const double* d_prev_u,
     if (precision == GG_PRECISION_MIXED) {
         H.mom32.ensure(sizeof(float) * nm * nel);
         H.kdiag32.ensure(sizeof(float) * nd);
-        GG_CUDA(cudaMemsetAsync(H.kdiag32.p, 0, sizeof(float) * nd, st));
         if (H.dim == 2)
             launch_build<2, float>(H, prev, d_prev_u, d_prev_p, H.mom32.as<float>(), H.kdiag32.as<float>(),
                                    nullptr, nullptr, false);

@@ -95,6 +95,7 @@ struct Handle {
 
     // operator
     DBuf mom64, mom32, kdiag64, kdiag32, sdiag, hvec, f;
+    DBuf kcorner, fcorner;  // per-element corner terms of the diagonal / force (build scratch)
     bool built = false;
     int built_precision = -1;
     DBuf prev_u, prev_p;  // previous solution read by the yield laws (SoA / element)

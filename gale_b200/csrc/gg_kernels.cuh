@@ -49,8 +49,10 @@ int dvc_update(Handle& H, const gg_pcdvc_params* prm, gg_pcdvc_stats* stats);
 int build_operator(Handle& H, int precision, int prev, const double* d_prev_u,
                    const double* d_prev_p);
 
-// y = K x on one level (level mesh mk, moments mom, bc mask); y is accumulated with
-// atomics and must be zero on entry; BC rows of y are left untouched (zero).
+// y = K x on one level (level mesh mk, moments mom, bc mask); y is accumulated and must
+// be zero on entry; BC rows of y are left untouched (zero).  FP64 sums every node's
+// element terms in a fixed order (one launch per element parity class: the same bits on
+// every run); FP32 accumulates with atomics in arrival order.
 // energy (nullable): per-block partials of Σ_e x_eᵀ K_e x_e.
 template <typename R>
 void apply_K(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
@@ -59,6 +61,8 @@ void apply_G(const Handle& H, const double* p, double* y, cudaStream_t st);
 void apply_GT(const Handle& H, const double* u, double* q, cudaStream_t st);
 
 // Krylov / Uzawa (gg_solve.cu)
+// Sizes the reduction scratch and clears its counters (before the first Krylov kernel).
+void prepare_krylov_scratch(Handle& H);
 int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& st);
 int inner_solve(Handle& H, const gg_uzawa_params& prm, const double* b, double* x,
                 double rtol, int maxit, int* iters, bool warm = false);

@@ -42,10 +42,39 @@ k_apply_K_small(MeshK mk, const float* __restrict__ mom, const uint8_t* __restri
     apply_tiles<DIM, float, 0, false, DIM == 3 ? 2 : 4, DIM == 3 ? 2 : 1>(mk, mom, bcmask, x, y, blockIdx.x, gridDim.x);
 }
 
+// One parity class of the FP64 apply (see apply_tiles_class): 2^dim launches in class
+// order make y = K x the same bits on every run.
+template <int DIM>
+__global__ void __launch_bounds__(256, 1)
+k_apply_K_class(MeshK mk, const double* __restrict__ mom, const uint8_t* __restrict__ bcmask,
+                const double* __restrict__ x, double* __restrict__ y, const int32_t* __restrict__ done, int color) {
+    if (done && *done) return;
+    apply_tiles_class<DIM, double, 0, false>(mk, mom, bcmask, x, y, blockIdx.x, gridDim.x, color);
+}
+
+int class_grid(const MeshK& mk, int color) {
+    const int64_t t = mk.dim == 3 ? class_tiles<3>(mk, color, ApplyTile<3>::X, ApplyTile<3>::Y, ApplyTile<3>::Z)
+                                  : class_tiles<2>(mk, color, ApplyTile<2>::X, ApplyTile<2>::Y, ApplyTile<2>::Z);
+    const int64_t cap = 8 * (int64_t)num_sms();
+    return (int)(t < 1 ? 1 : (t < cap ? t : cap));
+}
+
 template <typename R>
 void apply_K_ex(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
                 double* energy_part, int grid, cudaStream_t st, const int32_t* done) {
-    if constexpr (sizeof(R) == 4) {
+    if constexpr (sizeof(R) == 8) {
+        // FP64: fixed summation order, one launch per parity class.  No caller asks the
+        // FP64 apply for element energies (the FP64 CG has its own class kernels).
+        if (energy_part) throw CudaError(cudaErrorInvalidValue, "apply_K_ex<double> with energy", __FILE__, __LINE__);
+        const int ncls = 1 << mk.dim;
+        for (int c = 0; c < ncls; c++) {
+            if (mk.dim == 3)
+                k_apply_K_class<3><<<class_grid(mk, c), 256, 0, st>>>(mk, mom, bcmask, x, y, done, c);
+            else
+                k_apply_K_class<2><<<class_grid(mk, c), 256, 0, st>>>(mk, mom, bcmask, x, y, done, c);
+        }
+    } else {
+        // FP32 (multigrid, learned correction): atomics in arrival order
         if (!energy_part) {
             int64_t g = (mk.nel + 127) / 128;
             const int64_t cap = 16 * (int64_t)num_sms();
@@ -54,13 +83,8 @@ void apply_K_ex(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x
             else k_apply_K_small<2><<<(int)g, 128, 0, st>>>(mk, mom, bcmask, x, y, done);
             return;
         }
-    }
-    if (mk.dim == 2) {
-        if (energy_part) k_apply_K<2, R, true><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
-        else k_apply_K<2, R, false><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
-    } else {
-        if (energy_part) k_apply_K<3, R, true><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
-        else k_apply_K<3, R, false><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
+        if (mk.dim == 2) k_apply_K<2, R, true><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
+        else k_apply_K<3, R, true><<<grid, 256, 0, st>>>(mk, mom, bcmask, x, y, energy_part, done);
     }
 }
 template void apply_K_ex<double>(const MeshK&, const double*, const uint8_t*, const double*, double*,

@@ -24,6 +24,8 @@ __device__ __forceinline__ double block_sum(double v) {
 }
 
 int apply_grid(int64_t nel);
+// grid of one parity-class launch of the FP64 apply (apply_tiles_class)
+int class_grid(const MeshK& mk, int color);
 
 template <typename R>
 void apply_K_ex(const MeshK& mk, const R* mom, const uint8_t* bcmask, const R* x, R* y,
@@ -220,6 +222,50 @@ __device__ __forceinline__ double apply_tiles(const MeshK& mk, const R* __restri
         if (i < mk.n[0] && j < mk.n[1] && (DIM == 2 || k < mk.n[2]))
             en += element_apply_scatter<DIM, R, kLoad, kEnergy>(mk, mom, bcmask, x, y, i, j, k,
                                                                 i + mk.n[0] * (j + mk.n[1] * k));
+    }
+    return en;
+}
+
+// The FP64 apply is summed in a fixed order: elements are split into the 2^dim parity
+// classes color = (i&1) | (j&1)<<1 | (k&1)<<2, and one launch scatters one class.  Two
+// elements of the same class share no node, so every atomic of a launch lands on a node
+// no other thread of that launch touches, and each node receives its element terms in
+// class order 0, 1, …, 2^dim−1: y = ((0 + y_0) + y_1) + …, the same bits on every run.
+// The tile is taken in class coordinates (element i = 2·ci + (color&1), …), so a warp
+// still covers one x-row of 32 elements of its class.
+template <int DIM>
+__host__ __device__ __forceinline__ int class_extent(const MeshK& mk, int d, int color) {
+    return (mk.n[d] - ((color >> d) & 1) + 1) >> 1;
+}
+
+template <int DIM>
+inline int64_t class_tiles(const MeshK& mk, int color, int TX, int TY, int TZ) {
+    const int c0 = class_extent<DIM>(mk, 0, color), c1 = class_extent<DIM>(mk, 1, color);
+    const int c2 = DIM == 3 ? class_extent<DIM>(mk, 2, color) : 1;
+    return (int64_t)((c0 + TX - 1) / TX) * ((c1 + TY - 1) / TY) * ((c2 + TZ - 1) / TZ);
+}
+
+template <int DIM, typename R, int kLoad = 0, bool kEnergy = true, int TY = ApplyTile<DIM>::Y,
+          int TZ = ApplyTile<DIM>::Z>
+__device__ __forceinline__ double apply_tiles_class(const MeshK& mk, const R* __restrict__ mom,
+                                                    const uint8_t* __restrict__ bcmask, const R* __restrict__ x,
+                                                    R* __restrict__ y, int64_t tile0, int64_t tstride, int color) {
+    constexpr int TX = ApplyTile<DIM>::X;
+    const int px = color & 1, py = (color >> 1) & 1, pz = DIM == 3 ? (color >> 2) & 1 : 0;
+    const int c0 = class_extent<DIM>(mk, 0, color), c1 = class_extent<DIM>(mk, 1, color);
+    const int c2 = DIM == 3 ? class_extent<DIM>(mk, 2, color) : 1;
+    const int ntx = (c0 + TX - 1) / TX, nty = (c1 + TY - 1) / TY, ntz = (c2 + TZ - 1) / TZ;
+    const int32_t ntiles = ntx * nty * ntz;
+    const int tx = threadIdx.x % TX, ty = (threadIdx.x / TX) % TY, tz = threadIdx.x / (TX * TY);
+    double en = 0.0;
+    for (int32_t tile = (int32_t)tile0; tile < ntiles; tile += (int32_t)tstride) {
+        const int rr = tile / ntx;
+        const int ci = (tile - rr * ntx) * TX + tx, cj = (rr % nty) * TY + ty, ck = (rr / nty) * TZ + tz;
+        if (ci < c0 && cj < c1 && ck < c2) {
+            const int i = 2 * ci + px, j = 2 * cj + py, k = DIM == 3 ? 2 * ck + pz : 0;
+            en += element_apply_scatter<DIM, R, kLoad, kEnergy>(mk, mom, bcmask, x, y, i, j, k,
+                                                                i + mk.n[0] * (j + mk.n[1] * k));
+        }
     }
     return en;
 }

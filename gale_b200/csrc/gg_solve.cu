@@ -18,6 +18,7 @@
 
 #include <stdio.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "gg_internal.cuh"
@@ -172,6 +173,43 @@ k_cg_apply(MeshK mk, const V* __restrict__ mom, const uint8_t* __restrict__ bcma
             s->done = 1;
         }
     });
+}
+
+// The FP64 Ap = K p in a fixed summation order: one launch per element parity class
+// (apply_tiles_class), all with the same grid.  Each block's energy partial goes to
+// part[color·grid + block]; the last block of the last class sums the 2^dim·grid
+// partials in index order, so pᵀKp and α are the same bits on every run too.
+constexpr int kClassGridCap = 1280;
+
+template <int DIM>
+__global__ void __launch_bounds__(256, 1)
+k_cg_apply_class(MeshK mk, const double* __restrict__ mom, const uint8_t* __restrict__ bcmask,
+                 const double* __restrict__ p, double* __restrict__ Ap, KrylovScalars* s, double* part,
+                 unsigned int* counter, int color) {
+    if (s->done) return;
+    constexpr int NC = 1 << DIM;
+    double en = apply_tiles_class<DIM, double, 0, true>(mk, mom, bcmask, p, Ap, blockIdx.x, gridDim.x, color);
+    en = block_sum(en);
+    if (threadIdx.x == 0) part[color * gridDim.x + blockIdx.x] = en;
+    if (color != NC - 1) return;
+    __shared__ bool last;
+    __threadfence();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < NC * (int)gridDim.x; b += blockDim.x) acc += part[b];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        s->pAp = acc;
+        s->alpha = s->rz / acc;
+        if (!(acc > 0.0) || isinf(acc)) {
+            s->failed = 3;
+            s->done = 1;
+        }
+    }
 }
 
 // ---- flexible CG (truncated FCG) with a multigrid preconditioner ----------------------
@@ -343,11 +381,13 @@ struct Scratch {
 };
 
 static Scratch scratch(Handle& H) {
-    // [partials 4*kRedBlocks doubles][out 8 doubles][counters 8 uint]
-    H.red.ensure(sizeof(double) * (4 * kRedBlocks + 8) + sizeof(unsigned int) * 8);
+    // [partials kPart doubles][out 8 doubles][counters 8 uint]; kPart covers 4 partials of
+    // the vector kernels' grid and the 2^dim class launches of the FP64 CG apply
+    constexpr int kPart = 4 * kRedBlocks > 8 * kClassGridCap ? 4 * kRedBlocks : 8 * kClassGridCap;
+    H.red.ensure(sizeof(double) * (kPart + 8) + sizeof(unsigned int) * 8);
     Scratch s;
     s.part = H.red.as<double>();
-    s.out = s.part + 4 * kRedBlocks;
+    s.out = s.part + kPart;
     s.counter = reinterpret_cast<unsigned int*>(s.out + 8);
     return s;
 }
@@ -358,6 +398,8 @@ static void init_scratch(Handle& H) {
     H.scal.ensure(sizeof(KrylovScalars) * 2);
     if (!H.h_scal) GG_CUDA(cudaMallocHost(&H.h_scal, sizeof(KrylovScalars) * 2));
 }
+
+void prepare_krylov_scratch(Handle& H) { init_scratch(H); }
 
 static double dot(Handle& H, int64_t n, const double* a, const double* b) {
     Scratch s = scratch(H);
@@ -381,11 +423,23 @@ static void cg_iteration_kernels(Handle& H, const MeshK& mk, const V* mom, const
                                  const V* diag, V* x, V* r, V* z, V* p, V* Ap, KrylovScalars* ks,
                                  Scratch sc) {
     const int64_t n = (int64_t)mk.dim * mk.nnode;
-    const int ga = apply_grid(mk.nel);
-    if (mk.dim == 2)
-        k_cg_apply<2, V><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter);
-    else
-        k_cg_apply<3, V><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter + 1);
+    if constexpr (sizeof(V) == 8) {
+        int gc = 1;
+        for (int c = 0; c < (1 << mk.dim); c++) gc = std::max(gc, class_grid(mk, c));
+        gc = std::min(gc, kClassGridCap);
+        for (int c = 0; c < (1 << mk.dim); c++) {
+            if (mk.dim == 2)
+                k_cg_apply_class<2><<<gc, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter, c);
+            else
+                k_cg_apply_class<3><<<gc, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter + 1, c);
+        }
+    } else {
+        const int ga = apply_grid(mk.nel);
+        if (mk.dim == 2)
+            k_cg_apply<2, V><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter);
+        else
+            k_cg_apply<3, V><<<ga, 256, 0, H.stream>>>(mk, mom, bcmask, p, Ap, ks, sc.part, sc.counter + 1);
+    }
     k_cg_update<V><<<kRedBlocks, 256, 0, H.stream>>>(n, mk.nnode, bcmask, diag, x, r, z, p, Ap, ks,
                                                      sc.part, sc.counter + 2);
     k_cg_direction<V><<<grid_for(n, 256), 256, 0, H.stream>>>(n, z, p, ks);
@@ -793,7 +847,26 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     axpby(H, ne, -1.0, hv, 1.0, r);
     // STEP 4 (:664-837)
     double zr_prev = 1.0, absres = 0.0, relres = 0.0;
-    for (;;) {
+    bool exact = false;
+    {
+        // A velocity that already meets the constraint to rounding (boundary velocities
+        // that admit an exactly representable flow, found by the inner solve): r0 is then
+        // rounding noise whose constant-pressure part the Schur CG cannot remove, and the
+        // reference's loop would iterate on noise until α breaks down.  The solve ends at
+        // once with the current pressure (no outer iteration, relative residual 0).
+        double gmax = 0.0;
+        const int nen = 1 << H.dim;
+        for (int a = 0; a < nen; a++)
+            for (int c = 0; c < H.dim; c++) gmax = std::max(gmax, std::fabs(H.mk.Ge[a][c]));
+        const double floor_r = 64.0 * 2.220446049250313e-16 *
+                               (gmax * std::sqrt((double)nen) * std::sqrt(dot(H, nd, u, u)) + std::sqrt(dot(H, ne, hv, hv)));
+        const double r0 = std::sqrt(dot(H, ne, r, r));
+        if (r0 <= floor_r) {
+            exact = true;
+            absres = r0 / scaleq;
+        }
+    }
+    while (!exact) {
         if (prm.use_preconditioner) {
             k_div<<<grid_for(ne, 256), 256, 0, st>>>(ne, r, H.sdiag.as<double>(), qtmp);
             H.kernel_launches++;
@@ -835,6 +908,7 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
         const double chosen = prm.use_absolute_tolerance ? absres : relres;
         if (!((chosen > prm.tolerance) || (it < prm.min_iterations))) break;
     }
+    if (exact) relres = 0.0;
     S.outer_iterations = it;
     S.fallbacks = H.fallbacks;
     // the first solve after a build also accounts for the build's kernels

@@ -28,7 +28,11 @@ static int load(gg_handle** h, const gale_stokes_view* v) {
         rc = gg_create(&v->mesh, h);
         if (rc != GG_OK) return rc;
     }
-    if ((rc = gg_set_velocity_bc(*h, &v->bc)) != GG_OK) return rc;
+    if (v->bc_fixed)
+        rc = gg_set_velocity_bc_nodes(*h, v->bc_fixed, v->bc_values);
+    else
+        rc = gg_set_velocity_bc(*h, &v->bc);
+    if (rc != GG_OK) return rc;
     if ((rc = gg_set_materials(*h, v->n_materials, v->materials)) != GG_OK) return rc;
     if ((rc = gg_set_body_force(*h, &v->force)) != GG_OK) return rc;
     if ((rc = gg_set_temperature(*h, v->temperature)) != GG_OK) return rc;

@@ -30,6 +30,10 @@ typedef struct gale_stokes_view {
     const int32_t* material;         /* [n_points]                          */
     const double* plastic_strain;    /* [n_points] or NULL                  */
     const double* temperature;       /* nodal TemperatureField or NULL      */
+    /* per-node velocity conditions (VariableCondition_Apply at the nodes, condition
+       functions included); when set they replace `bc`                      */
+    const uint8_t* bc_fixed;         /* [nodes] bit c: component c fixed    */
+    const double* bc_values;         /* [nodes*dim] node-major              */
 } gale_stokes_view;
 
 /* Create (or reuse when *h is set) the handle, load the view, locate the points, build

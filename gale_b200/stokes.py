@@ -80,14 +80,26 @@ def VonMises(cohesion=0.0, cohesionAfterSoftening=0.0, minimumViscosity=0.0,
 def DruckerPrager(cohesion=0.0, cohesionAfterSoftening=0.0, frictionCoefficient=0.0,
                   frictionCoefficientAfterSoftening=0.0, minimumYieldStress=0.0,
                   minimumViscosity=0.0, maxStrainRate=0.0,
-                  strainWeakening=False) -> abi.Rheology:
-    """Underworld/Rheology/src/DruckerPrager.cxx:225-490 (XML defaults)."""
+                  strainWeakening=False, boundaryCohesion=0.0, boundaryCohesionAfterSoftening=0.0,
+                  boundaryFrictionCoefficient=0.0, boundaryFrictionCoefficientAfterSoftening=0.0,
+                  boundaryLeft=False, boundaryRight=False, boundaryBottom=False, boundaryTop=False,
+                  boundaryBack=False, boundaryFront=False, HydrostaticTerm=None) -> abi.Rheology:
+    """Underworld/Rheology/src/DruckerPrager.cxx:225-490 (XML defaults).  Elements in the
+    first or last layer along a wall flagged boundary<Wall> use the boundary cohesion and
+    friction (:341-361).  A HydrostaticTerm is refused by the library (GG_ERR_INVALID)."""
+    walls = sum(1 << i for i, on in enumerate((boundaryLeft, boundaryRight, boundaryBottom, boundaryTop,
+                                               boundaryBack, boundaryFront)) if on)
     return _rheo(abi.RHEO_DRUCKER_PRAGER, cohesion=cohesion,
                  cohesion_after_softening=cohesionAfterSoftening,
                  friction_coefficient=frictionCoefficient,
                  friction_coefficient_after_softening=frictionCoefficientAfterSoftening,
                  minimum_yield_stress=minimumYieldStress, minimum_viscosity=minimumViscosity,
-                 max_strain_rate=maxStrainRate, strain_weakening=int(strainWeakening))
+                 max_strain_rate=maxStrainRate, strain_weakening=int(strainWeakening),
+                 boundary_cohesion=boundaryCohesion,
+                 boundary_cohesion_after_softening=boundaryCohesionAfterSoftening,
+                 boundary_friction_coefficient=boundaryFrictionCoefficient,
+                 boundary_friction_coefficient_after_softening=boundaryFrictionCoefficientAfterSoftening,
+                 boundary_walls=walls, hydrostatic_term=int(HydrostaticTerm is not None))
 
 
 def Byerlee(cohesion=0.0, depthCoefficient=0.0, minimumViscosity=0.0) -> abi.Rheology:

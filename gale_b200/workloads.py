@@ -21,8 +21,8 @@ from typing import Any, List, Optional
 import numpy as np
 
 from . import abi
-from .stokes import (Arrhenius, BodyForce, DruckerPrager, FrankKamenetskii, MaterialViscosity,
-                     Mesh, RheologyMaterial, StrainWeakening, UzawaSolver, VelocityBC, free_slip,
+from .stokes import (Arrhenius, BodyForce, Byerlee, DruckerPrager, FrankKamenetskii, MaterialViscosity,
+                     Mesh, RheologyMaterial, StrainWeakening, UzawaSolver, VelocityBC, VonMises, free_slip,
                      Picard)
 
 
@@ -294,3 +294,55 @@ def viscous_suite(rheology: str):
             "Arrhenius": Arrhenius(eta0=1.0e-6, activationEnergy=27.63102112),
             "FrankKamenetskii": FrankKamenetskii(eta0=1.0e6, theta=13.815510558)}[rheology]
     return mesh, cell, xi, w, T, [RheologyMaterial([rheo])]
+
+
+def gauss_points(mesh: abi.MeshDesc, per_dim=2) -> np.ndarray:
+    """GaussParticleLayout (StgDomain/Swarm/src/GaussParticleLayout.cxx:175-180, default two
+    points per axis): the Gauss–Legendre abscissae of every element, element by element,
+    x fastest inside an element, mapped to global coordinates."""
+    if per_dim != 2:
+        raise ValueError("two Gauss points per axis only")
+    g = 1.0 / np.sqrt(3.0)
+    dim = mesh.dim
+    n = [mesh.elements[d] for d in range(dim)]
+    nel = int(np.prod(n))
+    e = np.repeat(np.arange(nel), 2 ** dim)
+    q = np.tile(np.arange(2 ** dim), nel)
+    idx = [e % n[0], (e // n[0]) % n[1]] + ([e // (n[0] * n[1])] if dim == 3 else [])
+    coords = np.empty((nel * 2 ** dim, dim))
+    for d in range(dim):
+        v = vertex_coords(mesh, d)
+        lo, hi = v[idx[d]], v[idx[d] + 1]
+        xi = np.where((q >> d) & 1, g, -g)
+        coords[:, d] = lo + 0.5 * (xi + 1.0) * (hi - lo)
+    return np.ascontiguousarray(coords)
+
+
+def yield_criterion_2d(kind: str, width=3.0, height=1.0) -> Workload:
+    """The model of the reference's yielding suites (Underworld/Rheology/tests/input/
+    testYieldCriterion.xml with testVonMisesYieldCriterion.xml or
+    testByerleeYieldCriterion.xml): 30×10 elements on [0, width]×[0, height], one material
+    of MaterialViscosity η = 3.4 followed by the yield rheology, a 2×2 Gauss particle layout,
+    Uzawa tolerance 1e-4 (VonMises deck) or 1e-5, and the IncompressibleExtensionBC
+    velocities: vx = +0.5 on the left wall and −0.5 on the right, vy = 0 on the bottom and
+    vy = height·(0.5 − (−0.5))/width on the top (Underworld/plugins/IncompressibleExtensionBC/
+    IncompressibleExtensionBC.cxx GetTopWallVelocity / GetBottomWallVelocity with
+    constantHeight 0), a pure-shear shortening whose stress invariant is 2·3.4/width.
+    VonMises: cohesion 3.0222222 (the whole box yields once width < 2.25); Byerlee: cohesion
+    2, depthCoefficient 0.533333333333333 (the upper half yields at width 3)."""
+    mesh = Mesh(2, (30, 10), (0.0, 0.0), (width, height))
+    left, right = 0.5, -0.5
+    top = -height * (right - left) / width
+    bc = VelocityBC(left={"vx": left}, right={"vx": right}, top={"vy": top}, bottom={"vy": 0.0})
+    if kind == "VonMises":
+        yr, tol = VonMises(cohesion=3.0222222), 1e-4
+    elif kind == "Byerlee":
+        yr, tol = Byerlee(cohesion=2.0, depthCoefficient=0.533333333333333), 1e-5
+    else:
+        raise ValueError(kind)
+    coords = gauss_points(mesh)
+    mats = [RheologyMaterial([MaterialViscosity(3.4), yr])]
+    return Workload(f"yield_criterion_{kind}", mesh, bc, mats, BodyForce(), coords,
+                    np.zeros(coords.shape[0], dtype=np.int32), uzawa=UzawaSolver(tolerance=tol),
+                    picard=Picard(nonLinearMaxIterations=500, nonLinearTolerance=0.01),
+                    meta={"width": width, "height": height})

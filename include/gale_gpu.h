@@ -98,6 +98,18 @@ typedef struct gg_rheology {
     double depth_coefficient;           /* Byerlee                                    */
     int32_t strain_rate_softening;      /* VonMises                                   */
     int32_t pad;
+    /* DruckerPrager boundary strength (DruckerPrager.cxx:225-247, 326-361, 448-490):
+     * an element in the first or last element layer along a wall whose bit is set in
+     * boundary_walls (bit w = wall w of the order above: left, right, bottom, top, back,
+     * front) uses these four in place of cohesion / friction_coefficient               */
+    double boundary_cohesion;
+    double boundary_cohesion_after_softening;
+    double boundary_friction_coefficient;
+    double boundary_friction_coefficient_after_softening;
+    int32_t boundary_walls;
+    /* nonzero: the deck attaches a HydrostaticTerm (DruckerPrager.cxx:327-332), which this
+     * library does not evaluate; gg_set_materials refuses it with GG_ERR_INVALID        */
+    int32_t hydrostatic_term;
 } gg_rheology;
 
 typedef struct gg_strain_weakening {    /* StrainWeakening.cxx:250-275                */

@@ -8,6 +8,7 @@
  */
 #include "gale_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -417,6 +418,10 @@ int or_set_velocity_bc_nodes(or_problem* P, const uint8_t* fixed, const double* 
 
 int or_set_materials(or_problem* P, int32_t n, const gg_material* mats) {
     if (n < 1 || n > GG_MAX_MATERIALS) return fail(GG_ERR_INVALID, "material count");
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < mats[i].n_rheologies && k < GG_MAX_RHEOLOGIES; k++)
+            if (mats[i].rheology[k].hydrostatic_term)
+                return fail(GG_ERR_INVALID, "DruckerPrager HydrostaticTerm is not supported");
     P->nmat = n;
     memcpy(P->mats, mats, sizeof(gg_material) * n);
     return GG_OK;
@@ -625,9 +630,18 @@ static double run_rheologies(const or_problem* P, int64_t p, int prev, const dou
                 crit = r->cohesion * (1.0 - ratio) + r->cohesion_after_softening * ratio;
             } else if (r->kind == GG_RHEO_DRUCKER_PRAGER) { /* DruckerPrager.cxx:296-412 */
                 double pressure = pres ? pres[P->cell[p]] : 0.0;
-                double mu = r->friction_coefficient * (1.0 - ratio) +
-                            r->friction_coefficient_after_softening * ratio;
-                double C = r->cohesion * (1.0 - ratio) + r->cohesion_after_softening * ratio;
+                /* inside_boundary (:341-361): the element touches a flagged wall */
+                int bw = r->boundary_walls;
+                int inb = ((bw & 1) && ijk[0] == 0) || ((bw & 2) && ijk[0] == M->n[0] - 1) ||
+                          ((bw & 4) && ijk[1] == 0) || ((bw & 8) && ijk[1] == M->n[1] - 1) ||
+                          (dim == 3 && (((bw & 16) && ijk[2] == 0) || ((bw & 32) && ijk[2] == M->n[2] - 1)));
+                /* _DruckerPrager_EffectiveFrictionCoefficient / _EffectiveCohesion (:448-490) */
+                double mu = inb ? r->boundary_friction_coefficient * (1.0 - ratio) +
+                                      r->boundary_friction_coefficient_after_softening * ratio
+                                : r->friction_coefficient * (1.0 - ratio) +
+                                      r->friction_coefficient_after_softening * ratio;
+                double C = inb ? r->boundary_cohesion * (1.0 - ratio) + r->boundary_cohesion_after_softening * ratio
+                               : r->cohesion * (1.0 - ratio) + r->cohesion_after_softening * ratio;
                 double factor, fs;
                 if (dim == 2) {
                     factor = 1 / sqrt(1 + mu * mu);
@@ -1036,10 +1050,21 @@ int or_moments(or_problem* P, double* mom, int32_t* nmom) {
 }
 
 /* ------------------------------------------------------------ solvers --- */
+/* Sum of 64 fixed chunks, each summed in index order, then the chunks in order: the
+ * same bits for any thread count and on every run (an OpenMP reduction clause combines
+ * the threads' partial sums in arrival order).                                       */
 static double dot(int64_t n, const double* a, const double* b) {
+    enum { kChunks = 64 };
+    double part[kChunks];
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < kChunks; c++) {
+        const int64_t lo = n * c / kChunks, hi = n * (c + 1) / kChunks;
+        double s = 0.0;
+        for (int64_t i = lo; i < hi; i++) s += a[i] * b[i];
+        part[c] = s;
+    }
     double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-    for (int64_t i = 0; i < n; i++) s += a[i] * b[i];
+    for (int c = 0; c < kChunks; c++) s += part[c];
     return s;
 }
 
@@ -1153,6 +1178,23 @@ int or_uzawa(or_problem* P, const gg_uzawa_params* prm, double* u, double* p, gg
     for (int64_t e = 0; e < ne; e++) r[e] -= P->h[e];
     double zr_prev = 1.0, absres = 0.0, relres = 0.0;
     int k = 0;
+    /* A velocity that already meets the constraint to rounding (the boundary velocities
+     * admit an exactly representable flow and the inner solve found it): r0 is rounding
+     * noise whose constant-pressure component the Schur CG cannot remove, so the
+     * reference's loop (:664-837) would iterate on noise until alpha breaks down.  Here
+     * the solve ends at once with q0 (no outer iteration, relative residual 0).          */
+    {
+        double gmax = 0.0;
+        for (int a = 0; a < M->nen; a++)
+            for (int c = 0; c < dim; c++) gmax = fmax(gmax, fabs(P->Ge[a][c]));
+        double floor_r = 64.0 * DBL_EPSILON * (gmax * sqrt((double)M->nen) * sqrt(dot(nd, uu, uu)) + sqrt(dot(ne, P->h, P->h)));
+        double r0 = sqrt(dot(ne, r, r));
+        if (r0 <= floor_r) {
+            S.abs_residual = r0 / scaleq;
+            S.rel_residual = 0.0;
+            goto summary;
+        }
+    }
     for (;;) {
         /* 4.1 z = Ĝ⁻¹ r (Ĝ diagonal for P0) */
         for (int64_t e = 0; e < ne; e++) qtmp[e] = prm->use_preconditioner ? r[e] / P->sdiag[e] : r[e];
@@ -1185,6 +1227,7 @@ int or_uzawa(or_problem* P, const gg_uzawa_params* prm, double* u, double* p, gg
     S.outer_iterations = k;
     S.rel_residual = relres;
     S.abs_residual = absres;
+summary:
     /* summary norms (:844-877) */
     {
         apply_GT(P, uu, qtmp);

@@ -48,8 +48,8 @@ def test_c_host_solves_like_python(tmp_path):
     G.build_operator("fp64")
     up, pp, st = G.solve(w.uzawa)
     outer = int(r.stdout.split()[1])
-    # same algorithm and stopping rule; the FP64 atomics of the K apply make two runs agree
-    # to the Uzawa tolerance level (rtol 1e-5 here), not bitwise
-    assert abs(outer - st["outer_iterations"]) <= 1
-    assert np.linalg.norm(uc - up) <= 1e-3 * np.linalg.norm(up)
-    assert np.linalg.norm(pc - pp) <= 1e-3 * np.linalg.norm(pp)
+    # the same library call on the same inputs from C and from Python: the FP64 path sums
+    # in a fixed order, so the two solves are the same bits
+    assert outer == st["outer_iterations"]
+    assert np.array_equal(uc, up)
+    assert np.array_equal(pc, pp)

@@ -12,12 +12,13 @@ import os
 import numpy as np
 import pytest
 
+from conftest import reference_dir
 from gale_b200 import checkpoint, h5lite, workloads
 from gale_b200.stokes import Mesh
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden", "lid_driven_pic2d.npz")
-REF_CKPT = "/root/reference/PICellerator/SysTest/RegressionTests/expected/LidDrivenPIC2D.xml"
+LID_CKPT = os.path.join("PICellerator", "SysTest", "RegressionTests", "expected", "LidDrivenPIC2D.xml")
 
 
 def test_round_trip_every_type(tmp_path):
@@ -61,8 +62,7 @@ def test_save_load_round_trip(tmp_path):
 
 
 def test_written_files_match_the_reference_files(tmp_path):
-    if not os.path.isdir(REF_CKPT):
-        pytest.skip("reference tree not present")
+    REF_CKPT = os.path.join(reference_dir(), LID_CKPT)
     g = checkpoint.load(REF_CKPT, 10)
     w = workloads.lid_driven_pic2d()
     checkpoint.save(str(tmp_path), 10, w.mesh, g["velocity"], g["pressure"], g["positions"], g["material_index"],
@@ -87,9 +87,7 @@ def test_reads_every_reference_hdf5_file():
     """Every HDF5 file the reference ships (266 regression checkpoints, both checkpoint
     format versions, layout messages of version 2 and 3) parses: datasets, groups, attributes."""
     import glob
-    files = sorted(glob.glob("/root/reference/**/*.h5", recursive=True))
-    if not files:
-        pytest.skip("reference tree not present")
+    files = sorted(glob.glob(os.path.join(reference_dir(), "**", "*.h5"), recursive=True))
     for path in files:
         f = h5lite.File(path)
         f.attrs()

@@ -32,12 +32,12 @@ import numpy as np
 import pytest
 from scipy.spatial import cKDTree
 
+from conftest import reference_dir
 from gale_b200 import layouts, workloads
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden", "lid_driven_pic2d.npz")
 GOLDEN_RT = os.path.join(HERE, "golden", "rayleigh_taylor_benchmark.npz")
-REF = "/root/reference"
 
 
 def golden():
@@ -118,8 +118,7 @@ def test_sobol_layout_is_the_reference_sequence():
 
 
 def test_golden_fixture_matches_the_reference_files():
-    if not os.path.isdir(REF):
-        pytest.skip("reference tree not present")
+    REF = reference_dir()
     import sys
     sys.path.insert(0, os.path.join(HERE, "golden"))
     import make_lid_driven_golden as M
@@ -174,8 +173,7 @@ def check_rt_against_golden(run, g):
 
 
 def test_rt_fixture_matches_the_reference_files():
-    if not os.path.isdir(REF):
-        pytest.skip("reference tree not present")
+    REF = reference_dir()
     import sys
     sys.path.insert(0, os.path.join(HERE, "golden"))
     import make_rayleigh_taylor_golden as M
