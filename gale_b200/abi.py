@@ -108,6 +108,9 @@ class UzawaStats(C.Structure):
         ("rel_residual", C.c_double), ("abs_residual", C.c_double), ("div_u", C.c_double),
         ("momentum_residual", C.c_double), ("solve_ms", C.c_double),
         ("kernel_launches", C.c_int64),
+        ("fused_launches", C.c_int32), ("fused_iterations", C.c_int32), ("fused_ms", C.c_double),
+        ("fused_bytes_per_iteration", C.c_double), ("fused_barriers_per_iteration", C.c_int32),
+        ("pad_stats", C.c_int32),
     ]
 
     def as_dict(self):
@@ -207,6 +210,7 @@ ABI_FUNCTIONS = {
     "gg_get_rhs": ([_P, _PD, _PD], C.c_int),
     "gg_get_diagonals": ([_P, _PD, _PD], C.c_int),
     "gg_time_apply": ([_P, C.c_int32, C.c_int32, _PD], C.c_int),
+    "gg_time_grid_barrier": ([C.c_int32, C.c_int32, _PD], C.c_int),
     "gg_locate_noalloc": ([C.POINTER(MeshDesc), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                            C.POINTER(C.c_int64), C.c_void_p, C.POINTER(C.c_char_p)], C.c_int),
     "gg_solve_batch": ([C.c_int32, C.POINTER(_P), C.POINTER(UzawaParams), C.c_int32, C.POINTER(_PD),

@@ -181,6 +181,8 @@ int gg_create(const gg_mesh_desc* mesh, gg_handle** out) {
         GG_CUDA(cudaStreamCreateWithFlags(&H.stream, cudaStreamNonBlocking));
         GG_CUDA(cudaEventCreate(&H.ev0));
         GG_CUDA(cudaEventCreate(&H.ev1));
+        GG_CUDA(cudaEventCreate(&H.evf0));
+        GG_CUDA(cudaEventCreate(&H.evf1));
         H.bcmask.ensure(H.nnode);
         H.bcval.ensure(sizeof(double) * H.ndof);
         GG_CUDA(cudaMemsetAsync(H.bcmask.p, 0, H.nnode, H.stream));
@@ -207,6 +209,8 @@ int gg_destroy(gg_handle* h) {
     if (H.h_scal) cudaFreeHost(H.h_scal);
     if (H.ev0) cudaEventDestroy(H.ev0);
     if (H.ev1) cudaEventDestroy(H.ev1);
+    if (H.evf0) cudaEventDestroy(H.evf0);
+    if (H.evf1) cudaEventDestroy(H.evf1);
     if (H.stream) cudaStreamDestroy(H.stream);
     delete h;
     return GG_OK;

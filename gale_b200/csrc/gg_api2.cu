@@ -472,6 +472,17 @@ int gg_get_integration_points(gg_handle* h, double* xi, double* weight) {
     return GG_OK;
 }
 
+int gg_time_grid_barrier(int32_t blocks_per_sm, int32_t iters, double* us_per_barrier) {
+    if (!us_per_barrier) return GG_ERR_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GG_ERR_NO_DEVICE;
+    try {
+        return gg::time_grid_barrier(blocks_per_sm, iters, us_per_barrier);
+    } catch (const gg::CudaError&) {
+        return GG_ERR_CUDA;
+    }
+}
+
 int gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_launch) {
     if (!h || !ms_per_launch || reps < 1) return GG_ERR_INVALID;
     Handle& H = h->H;

@@ -437,12 +437,104 @@ k_fcg_fused(const int4* __restrict__ tab, const float* __restrict__ b, float* x,
     }
 }
 
+// Algorithmic bytes of one iteration of the program: what each phase must read and write
+// once (FP32 vectors, moments, BC bytes, the dense coarse inverse), no cache effects.
+double program_bytes(const FusedTable& T, const std::vector<FusedPhase>& prog, int nm) {
+    auto ndof = [&](int l) { return (double)T.lv[l].mk.dim * (double)T.lv[l].mk.nnode; };
+    double b = 0.0;
+    for (const FusedPhase& P : prog) {
+        const int l = P.level;
+        const double n = ndof(l), f = 4.0;
+        switch (P.type) {
+            case PH_APPLY:
+            case PH_APPLY_P:  // x in, y out, moments, BC bytes
+                b += 2.0 * n * f + (double)T.lv[l].mk.nel * nm * f + (double)T.lv[l].mk.nnode;
+                break;
+            case PH_STEP:  // r, t, d, D⁻¹, x in; r, d, x, t out
+                b += 9.0 * n * f;
+                break;
+            case PH_STEP_DOTS:  // + the FCG residual and Ap
+                b += 11.0 * n * f;
+                break;
+            case PH_RESTRICT:  // fine r, t in; coarse b (and the Chebyshev start) out
+                b += 2.0 * n * f + ndof(l + 1) * f * (P.flag ? 6.0 : 1.0) + (double)T.lv[l + 1].mk.nnode;
+                break;
+            case PH_DENSE:
+                b += (double)T.coarse_n * T.coarse_n * f + 2.0 * T.coarse_n * f;
+                break;
+            case PH_PROLONG:  // coarse x in; fine x in and out, t out
+                b += ndof(l + 1) * f + 3.0 * n * f + (double)T.lv[l].mk.nnode;
+                break;
+            case PH_RESTART:  // b, t, D⁻¹, x in; r, d, x, t out
+                b += 8.0 * n * f;
+                break;
+            case PH_DIR:  // z, p in; p, Ap out
+                b += 4.0 * n * f;
+                break;
+            case PH_UPDATE:  // x, p, r, Ap, D⁻¹ in; x, r, level-0 r, d, z, t out
+                b += 11.0 * n * f;
+                break;
+            default:
+                break;
+        }
+    }
+    return b;
+}
+
 struct FusedLaunch {
     int max_blocks[4] = {0, 0, 0, 0};  // co-resident blocks per device, by DIM
     bool probed[4] = {false, false, false, false};
 };
 
 }  // namespace
+
+// `iters` grid barriers in a row (the persistent kernels' barrier, nothing else): the
+// cost of one phase boundary.
+__global__ void __launch_bounds__(256) k_barrier_loop(int iters, GridBarrier* gb, int* failed) {
+    unsigned int epoch = 0;
+    for (int i = 0; i < iters; i++)
+        if (!grid_barrier(gb, &epoch)) {
+            if (threadIdx.x == 0) atomicAdd(failed, 1);
+            return;
+        }
+}
+
+// Measurement only: microseconds per grid barrier over `iters` barriers of one cooperative
+// launch with `blocks_per_sm` blocks of 256 threads per SM (CUDA events).
+int time_grid_barrier(int blocks_per_sm, int iters, double* us) {
+    int dev = 0, per_sm = 0;
+    GG_CUDA(cudaGetDevice(&dev));
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_barrier_loop, 256, 0));
+    if (blocks_per_sm < 1 || blocks_per_sm > per_sm || iters < 1) return GG_ERR_INVALID;
+    int grid = blocks_per_sm * num_sms();
+    GridBarrier* gb = nullptr;
+    int* failed = nullptr;
+    GG_CUDA(cudaMalloc(&gb, sizeof(GridBarrier)));
+    GG_CUDA(cudaMalloc(&failed, sizeof(int)));
+    cudaEvent_t e0, e1;
+    GG_CUDA(cudaEventCreate(&e0));
+    GG_CUDA(cudaEventCreate(&e1));
+    float ms = 0.f;
+    int hf = 0;
+    for (int rep = 0; rep < 2; rep++) {  // the first launch warms up
+        GG_CUDA(cudaMemset(gb, 0, sizeof(GridBarrier)));
+        GG_CUDA(cudaMemset(failed, 0, sizeof(int)));
+        void* args[] = {(void*)&iters, (void*)&gb, (void*)&failed};
+        GG_CUDA(cudaEventRecord(e0, 0));
+        GG_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_loop, dim3(grid), dim3(256), args, 0, 0));
+        GG_CUDA(cudaEventRecord(e1, 0));
+        GG_CUDA(cudaEventSynchronize(e1));
+        GG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        GG_CUDA(cudaMemcpy(&hf, failed, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(gb);
+    cudaFree(failed);
+    if (hf) return GG_ERR_CUDA;
+    *us = (double)ms * 1e3 / iters;
+    return GG_OK;
+}
 
 // On unless the environment sets GALE_B200_FUSED_FCG=0, which selects the graph-captured
 // kernel sequence (read at every solve, so one process can compare both).
@@ -542,6 +634,7 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
         ph(PH_UPDATE, 0);
         if ((int)prog.size() > kMaxPhases) return 1;
         T.nphase = (int)prog.size();
+        H.fused_bytes_it = program_bytes(T, prog, H.nm);
         for (size_t q = 0; q < prog.size(); q++) T.ph[q] = prog[q];
         H.fused_host.assign(kTabWords * 16, 0);
         std::memcpy(H.fused_host.data(), &T, sizeof T);
@@ -570,11 +663,20 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
     void* args[] = {(void*)&tab, (void*)&b,      (void*)&x,   (void*)&p,    (void*)&Ap, (void*)&rtol,
                     (void*)&maxit, (void*)&ks, (void*)&part, (void*)&gb};
     const void* fn = dim == 2 ? (const void*)k_fcg_fused<2> : (const void*)k_fcg_fused<3>;
+    GG_CUDA(cudaEventRecord(H.evf0, H.stream));
     GG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kFusedBlock), args, 0, H.stream));
+    GG_CUDA(cudaEventRecord(H.evf1, H.stream));
     H.kernel_launches += 1;
     GG_CUDA(cudaMemcpyAsync(H.h_scal, ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, H.stream));
     GG_CUDA(cudaStreamSynchronize(H.stream));
     *iters = H.h_scal->iterations;
+    {
+        float ms = 0.f;
+        GG_CUDA(cudaEventElapsedTime(&ms, H.evf0, H.evf1));
+        H.fused_ms_acc += ms;
+        H.fused_launches_acc++;
+        H.fused_its_acc += H.h_scal->iterations;
+    }
     if (H.h_scal->failed == 4) {
         H.err = "fused multigrid solve: grid barrier timed out";
         return GG_ERR_CUDA;

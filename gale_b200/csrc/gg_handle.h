@@ -122,6 +122,12 @@ struct Handle {
     const float* fused_r = nullptr;  // FCG residual / preconditioned vector baked into it
     const float* fused_z = nullptr;
     int fused_phases = 0;            // grid barriers per iteration
+    double fused_bytes_it = 0.0;     // algorithmic bytes of one iteration (every phase)
+    // measurement of the persistent launches of the current Uzawa solve (events around
+    // each cooperative launch on the handle's stream)
+    cudaEvent_t evf0 = nullptr, evf1 = nullptr;
+    int fused_launches_acc = 0, fused_its_acc = 0;
+    double fused_ms_acc = 0.0;
     // dofs per block of the persistent kernel's grid: 256 for a problem solved alone; 1024
     // when gg_solve_batch runs it beside others (fewer blocks per problem, more problems
     // resident at once: 512 sinkers 94 -> 107 solves/s, a lone 256x64 problem 10 % slower)

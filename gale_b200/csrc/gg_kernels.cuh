@@ -88,6 +88,8 @@ int fcg_mg_solve(Handle& H, const float* b, float* x, double rtol, int maxit, in
 // hierarchy does not fit it (no dense coarse level, > 8 levels, degree outside 2..4).
 int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters);
 bool fused_fcg_enabled();
+// µs per grid barrier of the persistent kernels (measurement, gg_fused.cu)
+int time_grid_barrier(int blocks_per_sm, int iters, double* us);
 
 // Learned coarse correction (gg_learned.cu)
 bool learned_ready(Handle& H);

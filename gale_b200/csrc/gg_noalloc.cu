@@ -131,6 +131,12 @@ extern "C" GG_API int gg_locate_noalloc(const gg_mesh_desc* mesh, int64_t n_poin
         *msg = "gg_locate_noalloc: no CUDA device";
         return GG_ERR_NO_DEVICE;
     }
+    // an error the caller left pending is not this call's: report it, leave it in place
+    // (cudaPeekAtLastError does not clear it) and launch nothing
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        *msg = "gg_locate_noalloc: a CUDA error was pending before the call";
+        return GG_ERR_CUDA;
+    }
     if (dev < 0 || dev >= kMaxDevices) {
         *msg = "gg_locate_noalloc: device index beyond 64";
         return GG_ERR_INVALID;
@@ -161,21 +167,32 @@ extern "C" GG_API int gg_locate_noalloc(const gg_mesh_desc* mesh, int64_t n_poin
         *msg = "gg_locate_noalloc: cudaMemsetAsync failed";
         return GG_ERR_CUDA;
     }
+    // each launch is checked on its own, so a failure names the kernel that raised it
+    auto launched = [&](const char* what) {
+        if (cudaGetLastError() == cudaSuccess) return true;
+        *msg = what;
+        return false;
+    };
     k_locate<<<grid_of(n_points, 256), 256, 0, st>>>(mk, n_points, d_coords, d_cell, counts, flags);
+    if (!launched("gg_locate_noalloc: launch of the location kernel failed")) return GG_ERR_CUDA;
     k_scan_blocks<<<(int)nblk, 1024, 0, st>>>(counts, nel, d_offsets, sums);
+    if (!launched("gg_locate_noalloc: launch of the block scan failed")) return GG_ERR_CUDA;
     k_scan_sums<<<1, 1024, 0, st>>>(sums, nblk, sums + nblk);
+    if (!launched("gg_locate_noalloc: launch of the block-sum scan failed")) return GG_ERR_CUDA;
     k_scan_add<<<(int)nblk, 1024, 0, st>>>(d_offsets, nel, sums, sums + nblk);
+    if (!launched("gg_locate_noalloc: launch of the scan fix-up failed")) return GG_ERR_CUDA;
     if (cudaMemsetAsync(counts, 0, sizeof(int32_t) * (nel + 1), st) != cudaSuccess) {
         *msg = "gg_locate_noalloc: cudaMemsetAsync failed";
         return GG_ERR_CUDA;
     }
     k_scatter<<<grid_of(n_points, 256), 256, 0, st>>>(n_points, nel, d_cell, d_offsets, counts, d_order);
+    if (!launched("gg_locate_noalloc: launch of the scatter failed")) return GG_ERR_CUDA;
     k_segsort_inplace<<<grid_of(nel * 32, 128), 128, 0, st>>>(nel, d_offsets, d_order, flags);
+    if (!launched("gg_locate_noalloc: launch of the per-element sort failed")) return GG_ERR_CUDA;
     int32_t hflags[2] = {0, 0};
-    if (cudaGetLastError() != cudaSuccess ||
-        cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
-        *msg = "gg_locate_noalloc: CUDA error";
+        *msg = "gg_locate_noalloc: CUDA error while reading the flags";
         return GG_ERR_CUDA;
     }
     if (n_outside) *n_outside = hflags[0];

@@ -757,6 +757,9 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     const int maxit = prm.inner_max_iterations > 0 ? prm.inner_max_iterations : 10000;
     GG_CUDA(cudaEventRecord(H.ev0, st));
     const int64_t launches0 = H.kernel_launches;
+    H.fused_launches_acc = 0;
+    H.fused_its_acc = 0;
+    H.fused_ms_acc = 0.0;
     H.fallbacks = 0;
     H.nn_enabled = true;
     H.tight_sweeps = false;
@@ -911,6 +914,11 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     if (exact) relres = 0.0;
     S.outer_iterations = it;
     S.fallbacks = H.fallbacks;
+    S.fused_launches = H.fused_launches_acc;
+    S.fused_iterations = H.fused_its_acc;
+    S.fused_ms = H.fused_ms_acc;
+    S.fused_bytes_per_iteration = H.fused_launches_acc ? H.fused_bytes_it : 0.0;
+    S.fused_barriers_per_iteration = H.fused_launches_acc ? H.fused_phases : 0;
     // the first solve after a build also accounts for the build's kernels
     S.kernel_launches = H.kernel_launches - (H.stats_gen != H.build_gen ? H.launches_at_build : launches0);
     H.stats_gen = H.build_gen;

@@ -182,6 +182,16 @@ typedef struct gg_uzawa_stats {
     double  momentum_residual;    /* |f - K u - G p| / |f|                              */
     double  solve_ms;             /* device time of the solve                           */
     int64_t kernel_launches;      /* launches of this library's kernels in the solve    */
+    /* the persistent multigrid flexible-CG launches of the solve (mixed path): count,
+     * summed device time (CUDA events on the handle's stream around each launch), FCG
+     * iterations, grid barriers per iteration, and the algorithmic bytes of one iteration
+     * counting every phase of the V-cycle (vectors, moments, BC masks, coarse inverse)   */
+    int32_t fused_launches;
+    int32_t fused_iterations;
+    double  fused_ms;
+    double  fused_bytes_per_iteration;
+    int32_t fused_barriers_per_iteration;
+    int32_t pad_stats;
 } gg_uzawa_stats;
 
 typedef struct gg_picard_params {
@@ -273,7 +283,9 @@ GG_API int  gg_locate(gg_handle* h, uint32_t* owning_cell);
  * computed on device buffers the caller owns, without a handle and without any
  * allocation.  Inputs/outputs are device pointers: d_coords [n_points*dim], d_cell
  * [n_points] (element count for points outside), d_offsets [elements+1], d_order
- * [n_points] (point indices grouped by element, ascending inside each element).  Limits:
+ * [n_points] (point indices grouped by element, ascending inside each element; only
+ * d_order[0 .. d_offsets[elements]) is written, entries past it keep the caller's
+ * contents, one per point outside the mesh).  Limits:
  * at most 1,048,576 elements and 1024 points per element (GG_ERR_INVALID otherwise, with
  * *message set).  The counting-sort scratch is one fixed device array shared by every
  * call on a device: calls that overlap on the GPU race and must be serialised by the
@@ -414,6 +426,11 @@ GG_API int  gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const fl
 /* Measurement only (no reference counterpart): average device time of one matrix-free
  * K apply over `reps` back-to-back launches on the handle's stream, CUDA events.       */
 GG_API int  gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_launch);
+
+/* Measurement only (no reference counterpart): microseconds per grid barrier of the
+ * persistent kernels, `iters` barriers in one cooperative launch of `blocks_per_sm`
+ * blocks of 256 threads per SM on the current device (CUDA events, default stream).   */
+GG_API int  gg_time_grid_barrier(int32_t blocks_per_sm, int32_t iters, double* us_per_barrier);
 
 #ifdef __cplusplus
 }

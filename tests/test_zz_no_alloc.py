@@ -42,10 +42,13 @@ def call_noalloc(lib, mesh, coords, torch):
     outside = C.c_int64(-1)
     msg = C.c_char_p()
     torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
     rc = lib.gg_locate_noalloc(C.byref(mesh), n, d_coords.data_ptr(), d_cell.data_ptr(), d_off.data_ptr(),
                                d_order.data_ptr(), C.byref(outside), None, C.byref(msg))
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
     return (rc, d_cell.cpu().numpy().view(np.uint32), d_off.cpu().numpy(), d_order.cpu().numpy(),
-            outside.value, (msg.value or b"").decode())
+            outside.value, (msg.value or b"").decode(), free_before - free_after)
 
 
 @pytest.mark.parametrize("make", [lambda: workloads.creep_3d(n=16), lambda: workloads.sinker_2d(n=64)],
@@ -58,9 +61,11 @@ def test_noalloc_matches_gg_locate_twice(make):
     order_expect = np.argsort(expect, kind="stable").astype(np.int32)
     nel = w.nel
     off_expect = np.concatenate([[0], np.cumsum(np.bincount(expect, minlength=nel))]).astype(np.int32)
-    for _ in range(2):  # the second call reuses the scratch the first one left behind
-        rc, cell, off, order, outside, msg = call_noalloc(lib, w.mesh, w.coords, torch)
+    for k in range(2):  # the second call reuses the scratch the first one left behind
+        rc, cell, off, order, outside, msg, grown = call_noalloc(lib, w.mesh, w.coords, torch)
         assert rc == abi.GG_OK, msg
+        if k == 1:
+            assert grown == 0  # the device's free memory is the same after the call
         assert outside == 0
         assert np.array_equal(cell, expect)
         assert np.array_equal(off, off_expect)
@@ -75,13 +80,15 @@ def test_noalloc_outside_points_and_limits():
     x = np.ascontiguousarray(rng.uniform(-0.05, 1.05, size=(5000, 2)))
     expect = reference_cells(mesh, x)
     for _ in range(2):
-        rc, cell, off, order, outside, msg = call_noalloc(lib, mesh, x, torch)
+        rc, cell, off, order, outside, msg, grown = call_noalloc(lib, mesh, x, torch)
         assert rc == abi.GG_ERR_OUT_OF_DOMAIN
+        assert grown == 0
         assert np.array_equal(cell, expect)
         assert outside == int((expect == 32 * 32).sum()) > 0
         inside = expect < 32 * 32
         assert off[-1] == inside.sum()
         assert np.array_equal(order[:off[-1]], np.argsort(np.where(inside, expect, 1 << 30), kind="stable")[:off[-1]])
+        assert (order[off[-1]:] == -1).all()  # past the last element: the caller's contents
     # sizes beyond the fixed scratch are rejected with a message, nothing launched
     big = Mesh(2, (2048, 1024))
     msg = C.c_char_p()
