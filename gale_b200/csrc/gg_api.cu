@@ -405,6 +405,14 @@ static void download_nodal(Handle& H, const double* dsrc, const double* add, dou
     GG_CUDA(cudaStreamSynchronize(H.stream));
 }
 
+void download_solution(Handle& H, double* u, double* p) {
+    store_solution(H);
+    download_nodal(H, H.u.as<double>(), H.bcval.as<double>(), u);
+    GG_CUDA(cudaMemcpyAsync(p, H.q.p, sizeof(double) * H.nel, cudaMemcpyDeviceToHost, H.stream));
+    GG_CUDA(cudaStreamSynchronize(H.stream));
+    H.have_solution = true;
+}
+
 // Operator build + Dirichlet elimination; device previous solution pointers (nullable).
 int build_all(Handle& H, int precision, int prev, const double* d_u, const double* d_p) {
     H.launches_at_build = H.kernel_launches;

@@ -122,6 +122,9 @@ struct Handle {
     const float* fused_r = nullptr;  // FCG residual / preconditioned vector baked into it
     const float* fused_z = nullptr;
     int fused_phases = 0;            // grid barriers per iteration
+    // the batched CTA solver's own hierarchy (gg_cta.cu): level buffers and λ_max per level
+    std::vector<std::unique_ptr<MGLevel>> cta_levels;
+    DBuf cta_lam;
     double fused_bytes_it = 0.0;     // algorithmic bytes of one iteration (every phase)
     // measurement of the persistent launches of the current Uzawa solve (events around
     // each cooperative launch on the handle's stream)

@@ -107,6 +107,14 @@ int learned_train(Handle& H, const gg_learn_params& P, gg_learn_stats& st);
 
 // prev_u = u + BC values, prev_p = q (gg_api2.cu)
 void store_solution(Handle& H);
+// store_solution, then the nodal velocity with its boundary values and the element
+// pressure to host arrays (gg_api.cu)
+void download_solution(Handle& H, double* u, double* p);
+
+// Batched CTA solver (gg_cta.cu): one CTA per problem, one launch for the batch.
+bool cta_batch_supported(const gg_uzawa_params& prm);
+int cta_batch_solve(std::vector<Handle*>& hs, const gg_uzawa_params& prm, double* const* u_out,
+                    double* const* p_out, gg_uzawa_stats* stats, int32_t* status);
 
 // Advection (gg_advect.cu)
 int advect(Handle& H, double dt, int order, const double* d_u, double* d_out);
