@@ -472,6 +472,20 @@ int gg_get_integration_points(gg_handle* h, double* xi, double* weight) {
     return GG_OK;
 }
 
+int gg_check_grid_barrier_timeout(int32_t spin_limit, int32_t* blocks_gave_up) {
+    if (!blocks_gave_up) return GG_ERR_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GG_ERR_NO_DEVICE;
+    try {
+        int g = 0;
+        const int rc = gg::check_barrier_timeout(spin_limit, &g);
+        *blocks_gave_up = g;
+        return rc;
+    } catch (const gg::CudaError&) {
+        return GG_ERR_CUDA;
+    }
+}
+
 int gg_time_grid_barrier(int32_t blocks_per_sm, int32_t iters, double* us_per_barrier) {
     if (!us_per_barrier) return GG_ERR_INVALID;
     int dev = 0;

@@ -36,7 +36,10 @@ MeshK make_mesh(const gg_mesh_desc& d);
 
 namespace {
 
-constexpr int kCtaThreads = 256;
+// threads per CTA: 512 in 2D (≤ 128 registers, 16 warps per SM), 256 in 3D, where the FP64
+// element apply needs ~220 registers
+template <int DIM>
+constexpr int cta_threads() { return DIM == 2 ? 512 : 256; }
 constexpr int kCtaMaxLevels = 8;
 constexpr int kCtaDenseMax = 200;  // dofs of a coarsest level inverted in shared memory
 constexpr int kCtaMinCoarse = 4;   // coarsen while every axis is even and ≥ 4 elements
@@ -79,7 +82,7 @@ struct CtaParams {
 // ---- block-level helpers -------------------------------------------------------------
 // Sum over the block in a fixed order; every thread gets the value.
 __device__ __noinline__ double cta_sum(double v) {
-    __shared__ double s_red[kCtaThreads / 32];
+    __shared__ double s_red[32];
     __shared__ double s_tot;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -87,7 +90,7 @@ __device__ __noinline__ double cta_sum(double v) {
     if (lane == 0) s_red[wid] = v;
     __syncthreads();
     if (wid == 0) {
-        v = lane < kCtaThreads / 32 ? s_red[lane] : 0.0;
+        v = lane < (int)(blockDim.x >> 5) ? s_red[lane] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) s_tot = v;
@@ -963,7 +966,7 @@ __device__ __noinline__ void cta_solve_problem(const CtaProblem& P, const CtaPar
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kCtaThreads, 1)
+__global__ void __launch_bounds__(cta_threads<DIM>(), 1)
 k_batch_uzawa(const CtaProblem* __restrict__ probs, const int32_t* __restrict__ order, int n, CtaParams prm,
               int* next) {
     extern __shared__ float s_dense[];
@@ -1122,8 +1125,9 @@ int cta_batch_solve(std::vector<Handle*>& hs, const gg_uzawa_params& prm, double
         const size_t smem = sizeof(float) * kCtaDenseMax * kCtaDenseMax;
         const void* fn = dim == 2 ? (const void*)k_batch_uzawa<2> : (const void*)k_batch_uzawa<3>;
         GG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int threads = dim == 2 ? cta_threads<2>() : cta_threads<3>();
         int per_sm = 0;
-        GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kCtaThreads, smem));
+        GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
         int grid = std::max(1, per_sm) * num_sms();
         if (grid > n) grid = n;
         CtaParams cp{};
@@ -1140,9 +1144,9 @@ int cta_batch_solve(std::vector<Handle*>& hs, const gg_uzawa_params& prm, double
         GG_CUDA(cudaEventCreate(&e1));
         GG_CUDA(cudaEventRecord(e0, 0));
         if (dim == 2)
-            k_batch_uzawa<2><<<grid, kCtaThreads, smem, 0>>>(d_probs, d_order, n, cp, d_next);
+            k_batch_uzawa<2><<<grid, threads, smem, 0>>>(d_probs, d_order, n, cp, d_next);
         else
-            k_batch_uzawa<3><<<grid, kCtaThreads, smem, 0>>>(d_probs, d_order, n, cp, d_next);
+            k_batch_uzawa<3><<<grid, threads, smem, 0>>>(d_probs, d_order, n, cp, d_next);
         GG_CUDA(cudaGetLastError());
         GG_CUDA(cudaEventRecord(e1, 0));
         GG_CUDA(cudaEventSynchronize(e1));

@@ -499,6 +499,36 @@ __global__ void __launch_bounds__(256) k_barrier_loop(int iters, GridBarrier* gb
         }
 }
 
+// The barrier's give-up path: block 0 leaves without arriving, so every other block's wait
+// runs out after `spin_limit` polls; each records that it gave up and returns.
+__global__ void __launch_bounds__(256) k_barrier_abandoned(long long spin_limit, GridBarrier* gb, int* gave_up) {
+    unsigned int epoch = 0;
+    if (blockIdx.x == 0) return;
+    if (!grid_barrier(gb, &epoch, spin_limit) && threadIdx.x == 0) atomicAdd(gave_up, 1);
+}
+
+int check_barrier_timeout(int spin_limit, int* gave_up) {
+    int per_sm = 0;
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_barrier_abandoned, 256, 0));
+    if (per_sm < 1 || spin_limit < 1) return GG_ERR_INVALID;
+    const int grid = num_sms();
+    GridBarrier* gb = nullptr;
+    int* d_gave = nullptr;
+    GG_CUDA(cudaMalloc(&gb, sizeof(GridBarrier)));
+    GG_CUDA(cudaMalloc(&d_gave, sizeof(int)));
+    GG_CUDA(cudaMemset(gb, 0, sizeof(GridBarrier)));
+    GG_CUDA(cudaMemset(d_gave, 0, sizeof(int)));
+    long long lim = spin_limit;
+    void* args[] = {(void*)&lim, (void*)&gb, (void*)&d_gave};
+    GG_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_abandoned, dim3(grid), dim3(256), args, 0, 0));
+    GG_CUDA(cudaDeviceSynchronize());
+    GG_CUDA(cudaMemcpy(gave_up, d_gave, sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(gb);
+    cudaFree(d_gave);
+    // the status the persistent solver reports for a barrier that gave up
+    return *gave_up > 0 ? GG_ERR_CUDA : GG_OK;
+}
+
 // Measurement only: microseconds per grid barrier over `iters` barriers of one cooperative
 // launch with `blocks_per_sm` blocks of 256 threads per SM (CUDA events).
 int time_grid_barrier(int blocks_per_sm, int iters, double* us) {

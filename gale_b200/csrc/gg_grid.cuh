@@ -29,7 +29,8 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
 // (made visible to thread 0 by __syncthreads) before every read after the barrier.
 // Returns false (uniformly within the block) once any block has given up waiting; the
 // caller then leaves the kernel.
-__device__ __noinline__ bool grid_barrier(GridBarrier* gb, unsigned int* epoch) {
+__device__ __noinline__ bool grid_barrier(GridBarrier* gb, unsigned int* epoch,
+                                          long long spin_limit = kBarrierSpinLimit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -38,7 +39,7 @@ __device__ __noinline__ bool grid_barrier(GridBarrier* gb, unsigned int* epoch) 
         asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&gb->arrive), "r"(1u) : "memory");
         long long spins = 0;
         while (ld_acquire_gpu(&gb->arrive) < target) {
-            if (++spins > kBarrierSpinLimit || ((spins & 1023) == 0 && *(volatile int*)&gb->err)) {
+            if (++spins > spin_limit || ((spins & 1023) == 0 && *(volatile int*)&gb->err)) {
                 atomicExch(&gb->err, 1);
                 ok = 0;
                 break;

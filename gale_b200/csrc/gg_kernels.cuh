@@ -90,6 +90,8 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
 bool fused_fcg_enabled();
 // µs per grid barrier of the persistent kernels (measurement, gg_fused.cu)
 int time_grid_barrier(int blocks_per_sm, int iters, double* us);
+// the grid barrier's give-up path with a short limit (block 0 never arrives)
+int check_barrier_timeout(int spin_limit, int* gave_up);
 
 // Learned coarse correction (gg_learned.cu)
 bool learned_ready(Handle& H);

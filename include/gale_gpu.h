@@ -432,6 +432,13 @@ GG_API int  gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double*
  * blocks of 256 threads per SM on the current device (CUDA events, default stream).   */
 GG_API int  gg_time_grid_barrier(int32_t blocks_per_sm, int32_t iters, double* us_per_barrier);
 
+/* Test of the failure path (no reference counterpart): one cooperative launch of one block
+ * per SM in which block 0 leaves without arriving at the persistent kernels' grid barrier,
+ * so every other block's wait runs out after `spin_limit` polls.  Returns GG_ERR_CUDA, the
+ * status the persistent solver reports for a barrier that gave up, with the number of
+ * blocks that gave up; the context stays usable.                                       */
+GG_API int  gg_check_grid_barrier_timeout(int32_t spin_limit, int32_t* blocks_gave_up);
+
 #ifdef __cplusplus
 }
 #endif

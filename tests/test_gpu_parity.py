@@ -309,3 +309,18 @@ def test_failure_statuses():
     with pytest.raises(GaleError) as e:
         H.build_operator()
     assert e.value.code == abi.GG_ERR_STATE
+
+
+def test_grid_barrier_wait_runs_out_and_context_survives():
+    """The persistent kernels' barrier gives up after its poll limit: every block but the
+    one that never arrives reports it, the call returns GG_ERR_CUDA, and the next launch on
+    the same context runs normally."""
+    import ctypes as C
+    lib = abi.load_library()
+    gave = C.c_int32(-1)
+    rc = lib.gg_check_grid_barrier_timeout(1 << 14, C.byref(gave))
+    assert rc == abi.GG_ERR_CUDA
+    import torch
+    assert gave.value == torch.cuda.get_device_properties(0).multi_processor_count - 1
+    us = C.c_double(0)
+    assert lib.gg_time_grid_barrier(1, 1000, C.byref(us)) == abi.GG_OK and us.value > 0
