@@ -18,8 +18,8 @@
 //                     with a block barrier between classes: no two threads add into the same
 //                     node at once, and every node sums its element terms in class order, so
 //                     a problem solved here gives the same bits on every run.
-// Vectors live in global memory (L2-resident for these sizes) and are read through L2
-// (ld.global.cg) inside the launch.
+// Vectors live in global memory (L2-resident for these sizes); inside the launch they are
+// read with L1-cached loads, coherent within the CTA across its block barriers.
 #include <math.h>
 
 #include <algorithm>
@@ -101,8 +101,11 @@ __device__ __noinline__ double cta_sum(double v) {
     return v;
 }
 
+// Vectors written inside the launch are read with plain (L1-cached) loads: every value a
+// thread reads was written by a thread of the same CTA before a block barrier, which makes
+// it visible in L1; no read-only (non-coherent) load touches them.
 template <typename T>
-__device__ __forceinline__ T ldg_cg(const T* p) { return __ldcg(p); }
+__device__ __forceinline__ T ldg_cg(const T* p) { return __ldca(p); }
 
 __device__ __forceinline__ bool is_fixed(const uint8_t* bc, int64_t i, int64_t nnode) {
     const int c = (int)(i / nnode);
@@ -123,7 +126,7 @@ __device__ __noinline__ double cta_apply(const MeshK& mk, const R* mom, const ui
             const int ci = idx % c0, rr = idx / c0;
             const int cj = rr % c1, ck = rr / c1;
             const int i = 2 * ci + px, j = 2 * cj + py, k = DIM == 3 ? 2 * ck + pz : 0;
-            en += element_apply_scatter<DIM, R, 1, kEnergy>(mk, mom, bc, x, y, i, j, k,
+            en += element_apply_scatter<DIM, R, 2, kEnergy>(mk, mom, bc, x, y, i, j, k,
                                                             i + mk.n[0] * (j + mk.n[1] * k));
         }
         __syncthreads();
