@@ -25,13 +25,19 @@
 // Global reductions: each block writes one FP64 partial; after the barrier every block
 // sums all partials in block order.  Every block then holds the same value and takes the
 // same branch without a second barrier.
-// Vectors written inside the launch are read through L2 only (__ldcg): the L1 and
-// non-coherent paths are not kept coherent across blocks within a kernel.
+// Vectors written inside the launch are never read through the non-coherent (read-only)
+// path.  Reads that touch each value once go through L2 only (__ldcg); reads that reuse
+// values across threads of an SM (the apply's nodal gathers, the restriction's and
+// prolongation's neighbour reads) are cached weak loads through L1 (__ldca).  Those vectors
+// are written only in earlier phases, and the grid barrier's release/acquire pair, followed
+// by the block barrier, orders every such write before every later load of the grid.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 
 #include <cstring>
+#include <cstdint>
+#include <type_traits>
 #include <mutex>
 #include <vector>
 
@@ -85,7 +91,7 @@ struct FusedTable {
     int nlevels;   // levels 0..nlevels-1; the last one is solved by the dense inverse
     int nphase;    // phases of one iteration
     int coarse_n;
-    int pad;
+    int vec4;      // every vector of the table and the launch is 16-byte aligned
     const float* coarse_inv;
     FusedLevel lv[kFusedMaxLevels];
     FusedPhase ph[kMaxPhases];
@@ -111,79 +117,223 @@ __device__ __noinline__ double all_sum(const double* slot) {
     return v;
 }
 
+// Two block sums in one pass (thread 0 writes both partials).
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+    __shared__ double s_a[32], s_b[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+        s_a[wid] = a;
+        s_b[wid] = b;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        a = lane < (int)(blockDim.x >> 5) ? s_a[lane] : 0.0;
+        b = lane < (int)(blockDim.x >> 5) ? s_b[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+    }
+}
+
+__device__ __forceinline__ void put_partial2(double a, double b, double* slot_a, double* slot_b) {
+    block_sum2(a, b);
+    if (threadIdx.x == 0) {
+        __stcg(&slot_a[blockIdx.x], a);
+        __stcg(&slot_b[blockIdx.x], b);
+    }
+}
+
+// all_sum of two partial arrays at once
+__device__ __noinline__ void all_sum2(const double* slot_a, const double* slot_b, double& a, double& b) {
+    __shared__ double s_val[2];
+    a = 0.0;
+    b = 0.0;
+    for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) {
+        a += __ldcg(&slot_a[q]);
+        b += __ldcg(&slot_b[q]);
+    }
+    block_sum2(a, b);
+    if (threadIdx.x == 0) {
+        s_val[0] = a;
+        s_val[1] = b;
+    }
+    __syncthreads();
+    a = s_val[0];
+    b = s_val[1];
+    __syncthreads();
+}
+
 __device__ __forceinline__ int64_t gtid() { return blockIdx.x * (int64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * blockDim.x; }
 
-// t += A v on level L (element tiles block-strided); returns this thread's Σ v_eᵀ A_e v_e
-// when kEnergy
+// t += A v on level L; returns this thread's Σ v_eᵀ A_e v_e when kEnergy.  Element tiles
+// block-strided; a level with at most one work item per grid thread at DIM threads per
+// element (16³ and below on the 296-block grid) takes the component-split apply instead
+// (kEnergy is only asked on level 0).  Measured per phase on creep 64³: the 16³ and 8³
+// applies 4.4 → 3.7 and 4.3 → 3.1 µs; the 32³ level (1.3 items per thread) was slower
+// split, 5.0 → 5.6 µs.
 template <int DIM, bool kEnergy>
 __device__ __forceinline__ double phase_apply(const FusedLevel& L, const float* v, float* t) {
+    if (!kEnergy && (int64_t)DIM * L.mk.nel <= gstride()) {
+        apply_split<DIM, float, 1>(L.mk, L.mom, L.bc, v, t, gtid(), gstride());
+        return 0.0;
+    }
     return apply_tiles<DIM, float, 1, kEnergy>(L.mk, L.mom, L.bc, v, t, blockIdx.x, gridDim.x);
+}
+
+// Node-wise phases work on slices of W consecutive FP32 elements: W = 4 moves slice v
+// (elements 4v … 4v+3) as one float4, W = 1 element v.  Every load of a slice is
+// independent, so a float4 slice keeps four elements' loads in flight where a scalar
+// grid-stride loop waited for each element's L2 round trip in turn.  (Batching several
+// slices per thread turn was measured slower: the batch's registers spill beside the
+// kernel's 128.)
+template <int W>
+__device__ __forceinline__ void ld_cg(const float* p, int64_t v, float (&o)[W]) {
+    if constexpr (W == 4) {
+        const float4 q = __ldcg(reinterpret_cast<const float4*>(p) + v);
+        o[0] = q.x;
+        o[1] = q.y;
+        o[2] = q.z;
+        o[3] = q.w;
+    } else {
+        o[0] = __ldcg(p + v);
+    }
+}
+
+// data no thread writes during the launch (the inverse diagonals)
+template <int W>
+__device__ __forceinline__ void ld_ro(const float* p, int64_t v, float (&o)[W]) {
+    if constexpr (W == 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p) + v);
+        o[0] = q.x;
+        o[1] = q.y;
+        o[2] = q.z;
+        o[3] = q.w;
+    } else {
+        o[0] = __ldg(p + v);
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void st(float* p, int64_t v, const float (&o)[W]) {
+    if constexpr (W == 4)
+        reinterpret_cast<float4*>(p)[v] = make_float4(o[0], o[1], o[2], o[3]);
+    else
+        p[v] = o[0];
+}
+
+// body(width, v) over the n elements of a level vector: float4 slices when `vec`, then the
+// n mod 4 tail one element at a time
+template <class Body>
+__device__ __forceinline__ void for_slices(int64_t n, bool vec, Body body) {
+    const int64_t n4 = vec ? n >> 2 : 0;
+    for (int64_t v = gtid(); v < n4; v += gstride()) body(std::integral_constant<int, 4>(), v);
+    for (int64_t i = 4 * n4 + gtid(); i < n; i += gstride()) body(std::integral_constant<int, 1>(), i);
 }
 
 // r −= t, d = c1 d + c2 D⁻¹ r, x += d, t = 0
 template <int DIM>
-__device__ __forceinline__ void phase_cheb_step(const FusedLevel& L, int k) {
-    const int64_t n = (int64_t)DIM * L.mk.nnode;
+__device__ __forceinline__ void phase_cheb_step(const FusedLevel& L, int k, bool vec) {
     const float c1 = L.c1[k], c2 = L.c2[k];
-    float* xl = L.x;
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float rv = __ldcg(&L.r[i]) - __ldcg(&L.t[i]);
-        const float dv = c1 * __ldcg(&L.d[i]) + c2 * L.invd[i] * rv;
-        L.r[i] = rv;
-        L.d[i] = dv;
-        xl[i] = __ldcg(&xl[i]) + dv;
-        L.t[i] = 0.f;
-    }
+    for_slices((int64_t)DIM * L.mk.nnode, vec, [&](auto w, int64_t v) {
+        constexpr int W = decltype(w)::value;
+        float r[W], t[W], d[W], iv[W], x[W], z0[W];
+        ld_cg<W>(L.r, v, r);
+        ld_cg<W>(L.t, v, t);
+        ld_cg<W>(L.d, v, d);
+        ld_ro<W>(L.invd, v, iv);
+        ld_cg<W>(L.x, v, x);
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+            r[e] = r[e] - t[e];
+            d[e] = c1 * d[e] + c2 * iv[e] * r[e];
+            x[e] = x[e] + d[e];
+            z0[e] = 0.f;
+        }
+        st<W>(L.r, v, r);
+        st<W>(L.d, v, d);
+        st<W>(L.x, v, x);
+        st<W>(L.t, v, z0);
+    });
 }
 
 // the same step on level 0, finishing z, with the FCG partial sums r·z and z·Ap
 template <int DIM>
 __device__ __forceinline__ void phase_cheb_step_dots(const FusedLevel& L, int k, const float* Ap, double& rz,
-                                                     double& zap) {
-    const int64_t n = (int64_t)DIM * L.mk.nnode;
+                                                     double& zap, bool vec) {
     const float c1 = L.c1[k], c2 = L.c2[k];
-    float* z = L.x;
-    const float* rf = L.b;
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float rv = __ldcg(&L.r[i]) - __ldcg(&L.t[i]);
-        const float dv = c1 * __ldcg(&L.d[i]) + c2 * L.invd[i] * rv;
-        L.r[i] = rv;
-        L.d[i] = dv;
-        const float zv = __ldcg(&z[i]) + dv;
-        z[i] = zv;
-        L.t[i] = 0.f;
-        rz += (double)__ldcg(&rf[i]) * (double)zv;
-        zap += (double)zv * (double)__ldcg(&Ap[i]);
-    }
+    for_slices((int64_t)DIM * L.mk.nnode, vec, [&](auto w, int64_t v) {
+        constexpr int W = decltype(w)::value;
+        float r[W], t[W], d[W], iv[W], z[W], rf[W], ap[W], z0[W];
+        ld_cg<W>(L.r, v, r);
+        ld_cg<W>(L.t, v, t);
+        ld_cg<W>(L.d, v, d);
+        ld_ro<W>(L.invd, v, iv);
+        ld_cg<W>(L.x, v, z);
+        ld_cg<W>(L.b, v, rf);
+        ld_cg<W>(Ap, v, ap);
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+            r[e] = r[e] - t[e];
+            d[e] = c1 * d[e] + c2 * iv[e] * r[e];
+            z[e] = z[e] + d[e];
+            z0[e] = 0.f;
+            rz += (double)rf[e] * (double)z[e];
+            zap += (double)z[e] * (double)ap[e];
+        }
+        st<W>(L.r, v, r);
+        st<W>(L.d, v, d);
+        st<W>(L.x, v, z);
+        st<W>(L.t, v, z0);
+    });
 }
 
 // post-smoothing start from x: r = b − t (t = A x), d = D⁻¹r/θ, x += d, t = 0
 template <int DIM>
-__device__ __forceinline__ void phase_restart(const FusedLevel& L) {
-    const int64_t n = (int64_t)DIM * L.mk.nnode;
-    const float* bl = L.b;
-    float* xl = L.x;
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float rv = __ldcg(&bl[i]) - __ldcg(&L.t[i]);
-        const float dv = L.inv_theta * L.invd[i] * rv;
-        L.r[i] = rv;
-        L.d[i] = dv;
-        xl[i] = __ldcg(&xl[i]) + dv;
-        L.t[i] = 0.f;
-    }
+__device__ __forceinline__ void phase_restart(const FusedLevel& L, bool vec) {
+    const float th = L.inv_theta;
+    for_slices((int64_t)DIM * L.mk.nnode, vec, [&](auto w, int64_t v) {
+        constexpr int W = decltype(w)::value;
+        float b[W], t[W], iv[W], x[W], r[W], d[W], z0[W];
+        ld_cg<W>(L.b, v, b);
+        ld_cg<W>(L.t, v, t);
+        ld_ro<W>(L.invd, v, iv);
+        ld_cg<W>(L.x, v, x);
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+            r[e] = b[e] - t[e];
+            d[e] = th * iv[e] * r[e];
+            x[e] = x[e] + d[e];
+            z0[e] = 0.f;
+        }
+        st<W>(L.r, v, r);
+        st<W>(L.d, v, d);
+        st<W>(L.x, v, x);
+        st<W>(L.t, v, z0);
+    });
 }
 
 // b_C = Pᵀ (r − t)_L (zero on coarse BC dofs); when C is smoothed, its Chebyshev start:
-// r = b, d = D⁻¹b/θ, x = d, t = 0
+// r = b, d = D⁻¹b/θ, x = d, t = 0.  One thread per coarse node.  Node counts are below 2^31
+// on every level: 32-bit index arithmetic.  Neighbours past the mesh edge are read at the
+// clamped (valid) index with weight 0, so every load of a node is unconditional and all of
+// them can be in flight at once.
 template <int DIM>
 __device__ __forceinline__ void phase_restrict(const FusedLevel& L, const FusedLevel& C, bool start) {
     const MeshK& fk = L.mk;
     const MeshK& ck = C.mk;
-    for (int64_t N = gtid(); N < ck.nnode; N += gstride()) {
-        const int I = (int)(N % ck.nn[0]);
-        const int64_t rr = N / ck.nn[0];
-        const int J = (int)(rr % ck.nn[1]), K = DIM == 3 ? (int)(rr / ck.nn[1]) : 0;
+    const int32_t cnode = (int32_t)ck.nnode;
+    for (int32_t N = (int32_t)gtid(); N < cnode; N += (int32_t)gstride()) {
+        const int32_t I = N % ck.nn[0], rr = N / ck.nn[0];
+        const int32_t J = rr % ck.nn[1], K = DIM == 3 ? rr / ck.nn[1] : 0;
         float acc[DIM];
 #pragma unroll
         for (int c = 0; c < DIM; c++) acc[c] = 0.f;
@@ -194,9 +344,11 @@ __device__ __forceinline__ void phase_restrict(const FusedLevel& L, const FusedL
 #pragma unroll
                 for (int dx = -1; dx <= 1; dx++) {
                     const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
-                    if (i < 0 || j < 0 || k < 0 || i >= fk.nn[0] || j >= fk.nn[1] || k >= fk.nn[2]) continue;
-                    const float w = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
-                    const int64_t n = i + (int64_t)fk.nn[0] * (j + (int64_t)fk.nn[1] * k);
+                    const bool in = i >= 0 && j >= 0 && k >= 0 && i < fk.nn[0] && j < fk.nn[1] && k < fk.nn[2];
+                    const float w = in ? (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f) : 0.f;
+                    const int32_t n = min(max(i, 0), fk.nn[0] - 1) +
+                                      fk.nn[0] * (min(max(j, 0), fk.nn[1] - 1) +
+                                                  fk.nn[1] * (DIM == 3 ? min(max(k, 0), fk.nn[2] - 1) : 0));
 #pragma unroll
                     for (int c = 0; c < DIM; c++) {
                         const int64_t q = (int64_t)c * fk.nnode + n;
@@ -220,50 +372,116 @@ __device__ __forceinline__ void phase_restrict(const FusedLevel& L, const FusedL
     }
 }
 
-// x_L += P x_C (fine BC dofs untouched), t_L = 0
+// The same restriction with one warp per coarse node: lane q < 3^dim loads fine neighbour q,
+// the warp sums the weighted values with a butterfly (fixed order).  A thread per coarse
+// node issues its 27 neighbours' loads one after another, which on the small levels (a few
+// hundred coarse nodes, a few warps busy) made each restriction ≈10 µs of latency.
+template <int DIM>
+__device__ __forceinline__ void phase_restrict_warp(const FusedLevel& L, const FusedLevel& C, bool start) {
+    const MeshK& fk = L.mk;
+    const MeshK& ck = C.mk;
+    const int lane = threadIdx.x & 31;
+    constexpr int NQ = DIM == 3 ? 27 : 9;
+    const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = DIM == 3 ? lane / 9 - 1 : 0;
+    const float w = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+    for (int64_t N = gtid() >> 5; N < ck.nnode; N += gstride() >> 5) {
+        const int I = (int)(N % ck.nn[0]);
+        const int64_t rr = N / ck.nn[0];
+        const int J = (int)(rr % ck.nn[1]), K = DIM == 3 ? (int)(rr / ck.nn[1]) : 0;
+        float acc[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) acc[c] = 0.f;
+        const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
+        if (lane < NQ && i >= 0 && j >= 0 && k >= 0 && i < fk.nn[0] && j < fk.nn[1] && k < fk.nn[2]) {
+            const int64_t n = i + (int64_t)fk.nn[0] * (j + (int64_t)fk.nn[1] * k);
+#pragma unroll
+            for (int c = 0; c < DIM; c++) {
+                const int64_t q = (int64_t)c * fk.nnode + n;
+                acc[c] = w * (__ldcg(&L.r[q]) - __ldcg(&L.t[q]));
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < DIM; c++)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+        if (lane < DIM) {
+            const int c = lane;
+            const uint8_t bm = C.bc[N];
+            const int64_t q = (int64_t)c * ck.nnode + N;
+            const float bv = ((bm >> c) & 1) ? 0.f : acc[c];
+            C.b[q] = bv;
+            if (start) {
+                const float dv = C.inv_theta * C.invd[q] * bv;
+                C.r[q] = bv;
+                C.d[q] = dv;
+                C.x[q] = dv;
+                C.t[q] = 0.f;
+            }
+        }
+    }
+}
+
+// x_L += P x_C (fine BC dofs untouched), t_L = 0.  Each thread takes kProlongBatch fine
+// nodes per turn (n, n + stride, …) and issues all their coarse-corner loads before any
+// update, so one L2 round trip covers the batch.  A corner of weight 0 is the low corner
+// again (hi = lo), so every load is valid and unconditional.  32-bit index arithmetic.
+// The phase reads and writes each fine x value once, so no other thread reads it meanwhile.
+constexpr int kProlongBatch = 2;
+
 template <int DIM>
 __device__ __forceinline__ void phase_prolong(const FusedLevel& L, const FusedLevel& C) {
     float* xl = L.x;
     const MeshK& fk = L.mk;
     const MeshK& ck = C.mk;
-    for (int64_t n = gtid(); n < fk.nnode; n += gstride()) {
-        const int i = (int)(n % fk.nn[0]);
-        const int64_t rr = n / fk.nn[0];
-        const int j = (int)(rr % fk.nn[1]), k = DIM == 3 ? (int)(rr / fk.nn[1]) : 0;
-        const int idx[3] = {i, j, k};
-        int lo[3], hi[3];
-        float wl[3], wh[3];
+    const int32_t fnode = (int32_t)fk.nnode, stride = (int32_t)gstride();
+    for (int32_t n0 = (int32_t)gtid(); n0 < fnode; n0 += kProlongBatch * stride) {
+        float acc[kProlongBatch][DIM], xv[kProlongBatch][DIM];
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            if (d >= DIM || (idx[d] & 1) == 0) {
-                lo[d] = hi[d] = idx[d] >> 1;
-                wl[d] = 1.f;
-                wh[d] = 0.f;
-            } else {
-                lo[d] = idx[d] >> 1;
-                hi[d] = lo[d] + 1;
-                wl[d] = wh[d] = 0.5f;
+        for (int bt = 0; bt < kProlongBatch; bt++) {
+            const int32_t n = n0 + bt * stride;
+            if (n >= fnode) break;
+#pragma unroll
+            for (int c = 0; c < DIM; c++) xv[bt][c] = __ldcg(&xl[(int64_t)c * fk.nnode + n]);
+            const int32_t i = n % fk.nn[0], rr = n / fk.nn[0];
+            const int32_t j = rr % fk.nn[1], k = DIM == 3 ? rr / fk.nn[1] : 0;
+            const int idx[3] = {i, j, k};
+            int lo[3], hi[3];
+            float wl[3], wh[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                if (d >= DIM || (idx[d] & 1) == 0) {
+                    lo[d] = hi[d] = idx[d] >> 1;
+                    wl[d] = 1.f;
+                    wh[d] = 0.f;
+                } else {
+                    lo[d] = idx[d] >> 1;
+                    hi[d] = lo[d] + 1;
+                    wl[d] = wh[d] = 0.5f;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < DIM; c++) acc[bt][c] = 0.f;
+#pragma unroll
+            for (int q = 0; q < (1 << DIM); q++) {
+                const int I = (q & 1) ? hi[0] : lo[0], J = (q & 2) ? hi[1] : lo[1], K = (q & 4) ? hi[2] : lo[2];
+                const float w = ((q & 1) ? wh[0] : wl[0]) * ((q & 2) ? wh[1] : wl[1]) *
+                                (DIM == 3 ? ((q & 4) ? wh[2] : wl[2]) : 1.f);
+                const int32_t N = I + ck.nn[0] * (J + ck.nn[1] * K);
+#pragma unroll
+                for (int c = 0; c < DIM; c++) acc[bt][c] += w * __ldca(&C.x[(int64_t)c * ck.nnode + N]);
             }
         }
-        float acc[DIM];
 #pragma unroll
-        for (int c = 0; c < DIM; c++) acc[c] = 0.f;
+        for (int bt = 0; bt < kProlongBatch; bt++) {
+            const int32_t n = n0 + bt * stride;
+            if (n >= fnode) break;
+            const uint8_t bm = L.bc[n];
 #pragma unroll
-        for (int q = 0; q < (1 << DIM); q++) {
-            const int I = (q & 1) ? hi[0] : lo[0], J = (q & 2) ? hi[1] : lo[1], K = (q & 4) ? hi[2] : lo[2];
-            const float w = ((q & 1) ? wh[0] : wl[0]) * ((q & 2) ? wh[1] : wl[1]) *
-                            (DIM == 3 ? ((q & 4) ? wh[2] : wl[2]) : 1.f);
-            if (w == 0.f) continue;
-            const int64_t N = I + (int64_t)ck.nn[0] * (J + (int64_t)ck.nn[1] * K);
-#pragma unroll
-            for (int c = 0; c < DIM; c++) acc[c] += w * __ldcg(&C.x[(int64_t)c * ck.nnode + N]);
-        }
-        const uint8_t bm = L.bc[n];
-#pragma unroll
-        for (int c = 0; c < DIM; c++) {
-            const int64_t q = (int64_t)c * fk.nnode + n;
-            if (!((bm >> c) & 1)) xl[q] = __ldcg(&xl[q]) + acc[c];
-            L.t[q] = 0.f;
+            for (int c = 0; c < DIM; c++) {
+                const int64_t q = (int64_t)c * fk.nnode + n;
+                if (!((bm >> c) & 1)) xl[q] = xv[bt][c] + acc[bt][c];
+                L.t[q] = 0.f;
+            }
         }
     }
 }
@@ -284,11 +502,38 @@ __device__ __forceinline__ void phase_dense(int n, const float* A, const float* 
 // (update = true); then the level-0 Chebyshev start on r.  Returns this thread's Σ r².
 template <int DIM>
 __device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool update, float alpha, const float* b,
-                                                     float* x, float* p, float* Ap) {
+                                                     float* x, float* p, float* Ap, bool vec) {
     const int64_t nnode = L0.mk.nnode, n = (int64_t)DIM * nnode;
     float* r = L0.b;
     float* z = L0.x;
     double acc = 0.0;
+    if (update) {
+        const float th = L0.inv_theta;
+        for_slices(n, vec, [&](auto w, int64_t v) {
+            constexpr int W = decltype(w)::value;
+            float xv[W], pv[W], rv[W], ap[W], iv[W], d[W], z0[W];
+            ld_cg<W>(x, v, xv);
+            ld_cg<W>(p, v, pv);
+            ld_cg<W>(r, v, rv);
+            ld_cg<W>(Ap, v, ap);
+            ld_ro<W>(L0.invd, v, iv);
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+                xv[e] = xv[e] + alpha * pv[e];
+                rv[e] = rv[e] - alpha * ap[e];  // BC rows of Ap are zero
+                acc += (double)rv[e] * (double)rv[e];
+                d[e] = th * iv[e] * rv[e];
+                z0[e] = 0.f;
+            }
+            st<W>(x, v, xv);
+            st<W>(r, v, rv);
+            st<W>(L0.r, v, rv);
+            st<W>(L0.d, v, d);
+            st<W>(z, v, d);
+            st<W>(L0.t, v, z0);
+        });
+        return acc;
+    }
     for (int64_t i = gtid(); i < n; i += gstride()) {
         float rv;
         if (update) {
@@ -325,7 +570,8 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, fl
     double* p_zap = part + 2 * G;
     double* p_pap = part + 3 * G;
     unsigned int epoch = 0;
-    put_partial(phase_update_start<DIM>(L0, false, 0.f, b, x, p, Ap), p_rr);
+    const bool vec = T.vec4 != 0;
+    put_partial(phase_update_start<DIM>(L0, false, 0.f, b, x, p, Ap, vec), p_rr);
     if (!grid_barrier(gb, &epoch)) return false;
     const double rnorm0 = sqrt(all_sum(p_rr));
     const double tt = rtol * rnorm0;
@@ -346,17 +592,21 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, fl
                     put_partial(phase_apply<DIM, true>(L0, p, Ap), p_pap);
                     break;
                 case PH_STEP:
-                    phase_cheb_step<DIM>(L, P.k);
+                    phase_cheb_step<DIM>(L, P.k, vec);
                     break;
                 case PH_STEP_DOTS: {
                     double rzp = 0.0, zap = 0.0;
-                    phase_cheb_step_dots<DIM>(L, P.k, Ap, rzp, zap);
-                    put_partial(rzp, p_rz);
-                    put_partial(zap, p_zap);
+                    phase_cheb_step_dots<DIM>(L, P.k, Ap, rzp, zap, vec);
+                    put_partial2(rzp, zap, p_rz, p_zap);
                     break;
                 }
                 case PH_RESTRICT:
-                    phase_restrict<DIM>(L, T.lv[P.level + 1], P.flag != 0);
+                    // a warp per coarse node where the grid's warps outnumber a quarter of
+                    // the coarse nodes (every level below the first coarse one)
+                    if ((gstride() >> 5) * 4 >= T.lv[P.level + 1].mk.nnode)
+                        phase_restrict_warp<DIM>(L, T.lv[P.level + 1], P.flag != 0);
+                    else
+                        phase_restrict<DIM>(L, T.lv[P.level + 1], P.flag != 0);
                     break;
                 case PH_DENSE:
                     phase_dense(T.coarse_n, T.coarse_inv, L.b, L.x);
@@ -365,16 +615,25 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, fl
                     phase_prolong<DIM>(L, T.lv[P.level + 1]);
                     break;
                 case PH_RESTART:
-                    phase_restart<DIM>(L);
+                    phase_restart<DIM>(L, vec);
                     break;
                 case PH_DIR:
-                    for (int64_t i = gtid(); i < n; i += gstride()) {
-                        p[i] = __ldcg(&L0.x[i]) + beta * __ldcg(&p[i]);
-                        Ap[i] = 0.f;
-                    }
+                    for_slices(n, vec, [&](auto w, int64_t v) {
+                        constexpr int W = decltype(w)::value;
+                        float zv[W], pv[W], z0[W];
+                        ld_cg<W>(L0.x, v, zv);
+                        ld_cg<W>(p, v, pv);
+#pragma unroll
+                        for (int e = 0; e < W; e++) {
+                            pv[e] = zv[e] + beta * pv[e];
+                            z0[e] = 0.f;
+                        }
+                        st<W>(p, v, pv);
+                        st<W>(Ap, v, z0);
+                    });
                     break;
                 case PH_UPDATE:
-                    put_partial(phase_update_start<DIM>(L0, true, alpha, b, x, p, Ap), p_rr);
+                    put_partial(phase_update_start<DIM>(L0, true, alpha, b, x, p, Ap, vec), p_rr);
                     break;
                 default:
                     break;
@@ -382,8 +641,8 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, fl
             if (!grid_barrier(gb, &epoch)) return false;
             // scalars after the phases that end in a reduction (same value in every block)
             if (P.type == PH_STEP_DOTS) {
-                rz = all_sum(p_rz);
-                const double zap = all_sum(p_zap);
+                double zap;
+                all_sum2(p_rz, p_zap, rz, zap);
                 // truncated flexible CG (Notay 2000): β = −(z·Ap)/(pᵀAp), p = z on the first step
                 beta = it == 0 ? 0.f : (float)(-zap / pAp);
             } else if (P.type == PH_APPLY_P) {
@@ -607,7 +866,7 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
     const int max_blocks = fl[dev].max_blocks[dim];
     float* r = H.cgr32.as<float>();
     float* z = H.z32.as<float>();
-    if (H.fused_gen != H.mg_gen || H.fused_r != r || H.fused_z != z) {
+    if (H.fused_gen != H.mg_gen || H.fused_r != r || H.fused_z != z || H.fused_x != x || H.fused_b != b) {
         FusedTable T;
         std::memset(&T, 0, sizeof T);
         T.nlevels = (int)nl;
@@ -663,6 +922,13 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
         ph(PH_APPLY_P, 0);
         ph(PH_UPDATE, 0);
         if ((int)prog.size() > kMaxPhases) return 1;
+        auto a16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
+        bool al = a16(r) && a16(z) && a16(x) && a16(H.p32.p) && a16(H.Ap32.p);
+        for (size_t l = 0; l < nl; l++) {
+            const FusedLevel& F = T.lv[l];
+            al = al && a16(F.invd) && a16(F.b) && a16(F.x) && a16(F.r) && a16(F.d) && a16(F.t);
+        }
+        T.vec4 = al ? 1 : 0;
         T.nphase = (int)prog.size();
         H.fused_bytes_it = program_bytes(T, prog, H.nm);
         for (size_t q = 0; q < prog.size(); q++) T.ph[q] = prog[q];
@@ -673,6 +939,8 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
         H.fused_gen = H.mg_gen;
         H.fused_r = r;
         H.fused_z = z;
+        H.fused_x = x;
+        H.fused_b = b;
         H.fused_phases = T.nphase;
     }
     const int64_t n = H.ndof;

@@ -121,6 +121,8 @@ struct Handle {
     int64_t fused_gen = -2;  // mg_gen the table was written for
     const float* fused_r = nullptr;  // FCG residual / preconditioned vector baked into it
     const float* fused_z = nullptr;
+    const float* fused_x = nullptr;  // the launch's solution and right-hand side (alignment)
+    const float* fused_b = nullptr;
     int fused_phases = 0;            // grid barriers per iteration
     // the batched CTA solver's own hierarchy (gg_cta.cu): level buffers and λ_max per level
     std::vector<std::unique_ptr<MGLevel>> cta_levels;

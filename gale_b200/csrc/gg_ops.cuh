@@ -60,10 +60,12 @@ __device__ __forceinline__ int32_t local_node(int32_t n0, int32_t nn0, int32_t n
 // The arithmetic and scatter of one element, given its gathered nodal values m[c][a]
 // (corner a = (dx, dy, dz) bits) and moments M; `fixed` holds bit 8q + 4dx + c for the
 // Dirichlet components of the corners of row q.  Shared by every loader of the apply.
+// c_only ≥ 0 forms and scatters output component c_only alone (the transform and the
+// velocity gradients still use every component).
 template <int DIM, typename R, bool kEnergy>
 __device__ __forceinline__ double element_compute_scatter(const MeshK& mk, R (&m)[DIM][1 << DIM],
                                                           const R (&M)[n_moments<DIM>()], uint32_t fixed,
-                                                          R* __restrict__ y, int32_t n0) {
+                                                          R* __restrict__ y, int32_t n0, int c_only = -1) {
     constexpr int NS = 1 << DIM;
     constexpr int NR = NS / 2;
     const int64_t nnode = mk.nnode;
@@ -98,6 +100,7 @@ __device__ __forceinline__ double element_compute_scatter(const MeshK& mk, R (&m
     double energy = 0.0;
 #pragma unroll
     for (int c = 0; c < DIM; c++) {
+        if (c_only >= 0 && c != c_only) continue;
         R Q[NS];
 #pragma unroll
         for (int S = 0; S < NS; S++) Q[S] = R(0);
@@ -154,7 +157,7 @@ template <int DIM, typename R, int kLoad = 0, bool kEnergy = true>
 __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R* __restrict__ mom,
                                                         const uint8_t* __restrict__ bcmask,
                                                         const R* __restrict__ x, R* __restrict__ y, int i, int j,
-                                                        int k, int32_t e) {
+                                                        int k, int32_t e, int c_only = -1) {
     constexpr int NS = 1 << DIM;
     constexpr int NM = n_moments<DIM>();
     const int64_t nnode = mk.nnode, nel = mk.nel;
@@ -187,7 +190,7 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
     const R* Me = mom + e;
 #pragma unroll
     for (int q = 0; q < NM; q++) M[q] = Me[q * nel];
-    return element_compute_scatter<DIM, R, kEnergy>(mk, m, M, fixed, y, n0);
+    return element_compute_scatter<DIM, R, kEnergy>(mk, m, M, fixed, y, n0, c_only);
 }
 
 // Element tiles of one 256-thread block: 32 × 4 × 2 elements in 3D, 32 × 8 in 2D, x fastest
@@ -224,6 +227,24 @@ __device__ __forceinline__ double apply_tiles(const MeshK& mk, const R* __restri
                                                                 i + mk.n[0] * (j + mk.n[1] * k));
     }
     return en;
+}
+
+// y += K x with DIM threads per element: work item w = c·nel + e forms and scatters output
+// component c of element e.  For levels with fewer elements than a third of the grid's
+// threads, where one thread per element leaves most of the grid idle and the apply's time
+// is one element's dependency chain: the split shortens that chain to about a third.
+template <int DIM, typename R, int kLoad>
+__device__ __forceinline__ void apply_split(const MeshK& mk, const R* __restrict__ mom,
+                                            const uint8_t* __restrict__ bcmask, const R* __restrict__ x,
+                                            R* __restrict__ y, int64_t w0, int64_t wstride) {
+    const int32_t nel = (int32_t)mk.nel;
+    for (int32_t w = (int32_t)w0; w < DIM * nel; w += (int32_t)wstride) {
+        const int c = w / nel;
+        const int32_t e = w - c * nel;
+        const int32_t i = e % mk.n[0], r = e / mk.n[0];
+        const int32_t j = r % mk.n[1], k = DIM == 3 ? r / mk.n[1] : 0;
+        element_apply_scatter<DIM, R, kLoad, false>(mk, mom, bcmask, x, y, i, j, k, e, c);
+    }
 }
 
 // The FP64 apply is summed in a fixed order: elements are split into the 2^dim parity
