@@ -110,7 +110,7 @@ class UzawaStats(C.Structure):
         ("kernel_launches", C.c_int64),
         ("fused_launches", C.c_int32), ("fused_iterations", C.c_int32), ("fused_ms", C.c_double),
         ("fused_bytes_per_iteration", C.c_double), ("fused_barriers_per_iteration", C.c_int32),
-        ("pad_stats", C.c_int32),
+        ("uzawa_fused", C.c_int32),
     ]
 
     def as_dict(self):

@@ -20,8 +20,9 @@
 //
 // Grid barrier: an arrival counter in device memory; thread 0 of each block polls it with
 // an iteration limit.  When the limit expires it raises an error word; every block then
-// leaves at its next barrier, and the host reads failed = 4 (GG_ERR_CUDA).  The launch is cooperative, so the driver either makes every
-// block co-resident or refuses the launch.
+// leaves at its next barrier, and the host reads the error word and returns GG_ERR_CUDA.
+// The launch is cooperative, so the driver either makes every block co-resident or
+// refuses the launch.
 // Global reductions: each block writes one FP64 partial; after the barrier every block
 // sums all partials in block order.  Every block then holds the same value and takes the
 // same branch without a second barrier.
@@ -502,7 +503,7 @@ __device__ __forceinline__ void phase_dense(int n, const float* A, const float* 
 // (update = true); then the level-0 Chebyshev start on r.  Returns this thread's Σ r².
 template <int DIM>
 __device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool update, float alpha, const float* b,
-                                                     float* x, float* p, float* Ap, bool vec) {
+                                                     const double* b64, float* x, float* p, float* Ap, bool vec) {
     const int64_t nnode = L0.mk.nnode, n = (int64_t)DIM * nnode;
     float* r = L0.b;
     float* z = L0.x;
@@ -542,7 +543,7 @@ __device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool 
         } else {
             const int c = (int)(i / nnode);
             const bool fixed = (L0.bc[i - (int64_t)c * nnode] >> c) & 1;
-            rv = fixed ? 0.f : b[i];
+            rv = fixed ? 0.f : (b64 ? (float)__ldcg(&b64[i]) : __ldcg(&b[i]));
             x[i] = 0.f;
             p[i] = 0.f;
             Ap[i] = 0.f;
@@ -558,10 +559,20 @@ __device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool 
     return acc;
 }
 
-// The whole solve; returns false if a barrier gave up.
+// Outcome of one flexible-CG solve (identical in every block).
+struct FcgResult {
+    double rnorm0, rnorm, ttol, rz, pAp;
+    int iterations;
+    int failed;  // 0 converged, 1 iteration cap, 2 non-finite residual, 3 pᵀAp ≤ 0
+};
+
+// The whole solve of K32 x = b to ‖r‖ ≤ rtol‖b‖ from x = 0, within a launch whose barrier
+// count is `epoch`; b is FP32, or FP64 (b64 non-null: rounded to FP32 as it is read).
+// Uses part[0, 4·gridDim.x).  Returns false if a barrier gave up.
 template <int DIM>
-__device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, float* x, float* p, float* Ap,
-                                         double rtol, int maxit, KrylovScalars* ks, double* part, GridBarrier* gb) {
+__device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, const double* b64, float* x, float* p,
+                                         float* Ap, double rtol, int maxit, double* part, GridBarrier* gb,
+                                         unsigned int& epoch, FcgResult& res) {
     const FusedLevel& L0 = T.lv[0];
     const int64_t n = (int64_t)DIM * L0.mk.nnode;
     const int G = gridDim.x;
@@ -569,9 +580,8 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, fl
     double* p_rz = part + G;
     double* p_zap = part + 2 * G;
     double* p_pap = part + 3 * G;
-    unsigned int epoch = 0;
     const bool vec = T.vec4 != 0;
-    put_partial(phase_update_start<DIM>(L0, false, 0.f, b, x, p, Ap, vec), p_rr);
+    put_partial(phase_update_start<DIM>(L0, false, 0.f, b, b64, x, p, Ap, vec), p_rr);
     if (!grid_barrier(gb, &epoch)) return false;
     const double rnorm0 = sqrt(all_sum(p_rr));
     const double tt = rtol * rnorm0;
@@ -633,7 +643,7 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, fl
                     });
                     break;
                 case PH_UPDATE:
-                    put_partial(phase_update_start<DIM>(L0, true, alpha, b, x, p, Ap, vec), p_rr);
+                    put_partial(phase_update_start<DIM>(L0, true, alpha, b, b64, x, p, Ap, vec), p_rr);
                     break;
                 default:
                     break;
@@ -668,17 +678,13 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, fl
             }
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ks->rnorm0 = rnorm0;
-        ks->rnorm = rn;
-        ks->ttol = ttol;
-        ks->rz = rz;
-        ks->pAp = pAp;
-        ks->iterations = it;
-        ks->failed = failed;
-        ks->maxit = maxit;
-        ks->done = 1;
-    }
+    res.rnorm0 = rnorm0;
+    res.rnorm = rn;
+    res.ttol = ttol;
+    res.rz = rz;
+    res.pAp = pAp;
+    res.iterations = it;
+    res.failed = failed;
     return true;
 }
 
@@ -690,10 +696,402 @@ k_fcg_fused(const int4* __restrict__ tab, const float* __restrict__ b, float* x,
     for (int i = threadIdx.x; i < kTabWords; i += blockDim.x) s_tab[i] = tab[i];
     __syncthreads();
     const FusedTable& T = *reinterpret_cast<const FusedTable*>(s_tab);
-    if (!fcg_body<DIM>(T, b, x, p, Ap, rtol, maxit, ks, part, gb) && threadIdx.x == 0) {
-        ks->failed = 4;
+    unsigned int epoch = 0;
+    FcgResult res;
+    // a barrier that gave up is reported by the barrier's own error word (read by the host)
+    if (fcg_body<DIM>(T, b, nullptr, x, p, Ap, rtol, maxit, part, gb, epoch, res) && blockIdx.x == 0 &&
+        threadIdx.x == 0) {
+        ks->rnorm0 = res.rnorm0;
+        ks->rnorm = res.rnorm;
+        ks->ttol = res.ttol;
+        ks->rz = res.rz;
+        ks->pAp = res.pAp;
+        ks->iterations = res.iterations;
+        ks->failed = res.failed;
+        ks->maxit = maxit;
         ks->done = 1;
     }
+}
+
+// ---- the whole Uzawa solve as one launch ---------------------------------------------
+// Stokes_SLE_UzawaSolver_Solve (StgFEM/SLE/ProvidedSystems/StokesFlow/src/
+// Stokes_SLE_UzawaSolver.cxx:393-938) on the mixed path: the outer conjugate-gradient loop
+// on the pressure, and each inner velocity solve as FP64 defect correction around the
+// multigrid flexible CG above (fcg_body).  The steps and stopping rules are those of
+// uzawa_solve / inner_solve in gg_solve.cu, which the host runs one kernel at a time
+// with a device-to-host read after every reduction; here every reduction is a grid
+// barrier and every block takes the same branches on the same values, so the solve
+// returns to the host once.  The FP64 K apply sums each node's element terms in parity-
+// class order (one phase per class) as apply_K<double> does.
+
+// Where a solve stopped early: the step whose status it returns.
+enum : int {
+    UZ_NONE = 0,
+    UZ_FIRST_INNER = 1,  // K u* = f
+    UZ_RHS = 2,          // ‖Gᵀu* − h‖ not finite
+    UZ_VELOCITY = 3,     // K u = f − G p
+    UZ_INNER_DIR = 4,    // K u* = G s
+    UZ_STEP = 5,         // z·r, s·Gᵀu*, α not finite
+    UZ_RESIDUAL = 6,     // ‖r‖ not finite
+    UZ_LIMIT = 7,        // outer iteration limit
+};
+
+struct UzawaFusedOut {
+    int status;            // GG_OK or a GG_ERR code
+    int where;             // UZ_*
+    int outer_iterations;
+    int inner_iterations;  // flexible-CG iterations of all inner solves
+    int inner_solves;
+    int sweeps;            // FP32 flexible-CG solves (defect-correction sweeps)
+    int pad[2];
+    double rel_residual, abs_residual;
+};
+
+struct UzawaFusedArgs {
+    const double* mom64;
+    const double* kdiag;  // FP64 diagonal of K (the inner stopping norm ‖D⁻¹r‖)
+    const double* sdiag;  // Ĝ, the pressure preconditioner's diagonal
+    const double* f;
+    const double* hv;
+    double *u, *vstar, *ftmp, *q, *qtmp, *r, *s, *r64;
+    float *e32, *p32, *Ap32;
+    double tolerance, inner_rtol, scaleq;
+    double floor_u, floor_h;  // the exact-flow test: ‖r0‖ ≤ floor_u ‖u‖ + floor_h ‖h‖
+    int max_iterations, min_iterations, use_abs, use_precond, recycle, inner_maxit, sweep_cap;
+    int pad;
+    UzawaFusedOut* out;
+    double* part;  // 8 · gridDim.x doubles
+    GridBarrier* gb;
+};
+
+// r64 = K x (r64 zero on entry): one phase per element parity class, so every node sums
+// its element terms in class order.  False if a barrier gave up.
+template <int DIM>
+__device__ __forceinline__ bool uz_apply_K64(const FusedTable& T, const UzawaFusedArgs& A, const double* x,
+                                             unsigned int& epoch) {
+    const FusedLevel& L0 = T.lv[0];
+#pragma unroll 1
+    for (int color = 0; color < (1 << DIM); color++) {
+        apply_tiles_class<DIM, double, 1, false>(L0.mk, A.mom64, L0.bc, x, A.r64, blockIdx.x, gridDim.x, color);
+        if (!grid_barrier(A.gb, &epoch)) return false;
+    }
+    return true;
+}
+
+// r64 = b − r64 on free rows (0 on Dirichlet rows); returns ‖D⁻¹ r64‖ (every block the
+// same value).  *ok = false if the barrier gave up.
+template <int DIM>
+__device__ __forceinline__ double uz_defect(const FusedTable& T, const UzawaFusedArgs& A, const double* b,
+                                            unsigned int& epoch, bool* ok) {
+    const FusedLevel& L0 = T.lv[0];
+    const int64_t nnode = L0.mk.nnode;
+    double* P = A.part + 4 * gridDim.x;
+    double acc = 0.0;
+    for (int64_t n = gtid(); n < nnode; n += gstride()) {
+        const uint8_t bm = L0.bc[n];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) {
+            const int64_t i = (int64_t)c * nnode + n;
+            double rv = 0.0;
+            if (!((bm >> c) & 1)) {
+                rv = __ldcg(&b[i]) - __ldcg(&A.r64[i]);
+                const double zv = rv / A.kdiag[i];
+                acc += zv * zv;
+            }
+            A.r64[i] = rv;
+        }
+    }
+    put_partial(acc, P);
+    *ok = grid_barrier(A.gb, &epoch);
+    return *ok ? sqrt(all_sum(P)) : 0.0;
+}
+
+constexpr int kUzBarrierFail = -1;
+
+// K x = b to ‖D⁻¹(b − Kx)‖ ≤ rtol ‖D⁻¹b‖ (inner_solve's mixed branch): FP32 multigrid
+// flexible-CG sweeps on the FP64 defect, each followed by x += e and the FP64 defect.
+// warm: start from x (else x = 0).  Returns GG_OK / GG_ERR_NOT_CONVERGED /
+// GG_ERR_NONFINITE, or kUzBarrierFail.
+template <int DIM>
+__device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArgs& A, const double* b, double* x,
+                                        double rtol, bool warm, bool& tight, unsigned int& epoch, int& its,
+                                        int& sweeps) {
+    const FusedLevel& L0 = T.lv[0];
+    const int64_t nnode = L0.mk.nnode;
+    double* P = A.part + 4 * gridDim.x;
+    // x = 0 and r = b on free rows (the defect of x = 0), or r = 0 for the apply to
+    // accumulate K x0 (warm); the partials of ‖D⁻¹b‖ on free rows either way
+    double acc = 0.0;
+    for (int64_t n = gtid(); n < nnode; n += gstride()) {
+        const uint8_t bm = L0.bc[n];
+#pragma unroll
+        for (int c = 0; c < DIM; c++) {
+            const int64_t i = (int64_t)c * nnode + n;
+            const bool fixed = (bm >> c) & 1;
+            const double bv = fixed ? 0.0 : __ldcg(&b[i]);
+            if (!fixed) {
+                const double zv = bv / A.kdiag[i];
+                acc += zv * zv;
+            }
+            if (!warm) x[i] = 0.0;
+            A.r64[i] = warm ? 0.0 : bv;
+        }
+    }
+    put_partial(acc, P);
+    if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
+    const double rnorm0 = sqrt(all_sum(P));
+    double ttol = rtol * rnorm0;
+    if (ttol < 1e-50) ttol = 1e-50;
+    double rn_cur = rnorm0;
+    if (!warm && rnorm0 <= ttol) return GG_OK;
+    // sweep −1 is the warm start's defect; every later turn is an FP32 sweep, x += e and
+    // the FP64 defect (one call site of the FP64 apply and the flexible CG each)
+    int total = 0;
+    int rc = GG_ERR_NOT_CONVERGED;
+    for (int sweep = warm ? -1 : 0; sweep < 50; sweep++) {
+        if (sweep >= 0) {
+            const double inner_rtol = tight ? 1e-5 : 1e-4;
+            const double srtol = fmax(inner_rtol, fmin(0.5, ttol / rn_cur));
+            FcgResult res;
+            if (!fcg_body<DIM>(T, nullptr, A.r64, A.e32, A.p32, A.Ap32, srtol, A.sweep_cap, A.part, A.gb, epoch,
+                               res))
+                return kUzBarrierFail;
+            total += res.iterations;
+            sweeps++;
+            if (res.failed >= 2) {
+                rc = GG_ERR_NONFINITE;
+                break;
+            }
+            // x += e, r = 0 for the apply
+            for (int64_t i = gtid(); i < (int64_t)DIM * nnode; i += gstride()) {
+                x[i] = __ldcg(&x[i]) + (double)__ldcg(&A.e32[i]);
+                A.r64[i] = 0.0;
+            }
+            if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
+        }
+        if (!uz_apply_K64<DIM>(T, A, x, epoch)) return kUzBarrierFail;
+        bool ok = true;
+        const double rn = uz_defect<DIM>(T, A, b, epoch, &ok);
+        if (!ok) return kUzBarrierFail;
+        if (!(rn == rn)) {
+            rc = GG_ERR_NONFINITE;
+            break;
+        }
+        if (sweep >= 2) tight = true;
+        if (rn <= ttol) {
+            rc = GG_OK;
+            break;
+        }
+        rn_cur = rn;
+        if (sweep >= 0 && total >= A.inner_maxit) break;
+    }
+    its += total;
+    return rc;
+}
+
+// The solve is written around ONE call of the inner solve (stage 1: K u* = f; stage 2:
+// K u = f − G p; stage 3: K u* = G s, once per outer iteration), so the flexible CG is
+// inlined once and keeps the kernel's registers.
+template <int DIM>
+__device__ __forceinline__ bool uzawa_body(const FusedTable& T, const UzawaFusedArgs& A, UzawaFusedOut& o) {
+    const FusedLevel& L0 = T.lv[0];
+    const MeshK& mk = L0.mk;
+    const int64_t nnode = mk.nnode, nel = mk.nel;
+    const int G = gridDim.x;
+    double* P0 = A.part + 4 * G;
+    double* P1 = A.part + 5 * G;
+    double* P2 = A.part + 6 * G;
+    unsigned int epoch = 0;
+    bool tight = false;
+    o.status = GG_OK;
+    o.where = UZ_NONE;
+    o.outer_iterations = 0;
+    o.inner_iterations = 0;
+    o.inner_solves = 0;
+    o.sweeps = 0;
+    o.rel_residual = 0.0;
+    o.abs_residual = 0.0;
+    int it = 0, stage = 1;
+    double rhs_scale = 0.0, absres = 0.0, relres = 0.0, zr = 0.0, zr_prev = 1.0;
+    bool exact = false;
+    // the inner solve of the current stage
+    const double* ib = A.f;  // STEP 1 (:553-565)
+    double* ix = A.vstar;
+    double irtol = A.tolerance;
+    bool iwarm = false;
+    for (;;) {
+        o.inner_solves++;
+        const int rc = uz_inner<DIM>(T, A, ib, ix, irtol, iwarm, tight, epoch, o.inner_iterations, o.sweeps);
+        if (rc == kUzBarrierFail) return false;
+        if (rc != GG_OK) {
+            o.status = rc;
+            o.where = stage == 1 ? UZ_FIRST_INNER : stage == 2 ? UZ_VELOCITY : UZ_INNER_DIR;
+            o.outer_iterations = it;
+            return true;
+        }
+        if (stage == 1) {
+            // Gᵀu* − h and its norm
+            double acc = 0.0;
+            for (int64_t e = gtid(); e < nel; e += gstride()) {
+                const double qv = -__ldcg(&A.hv[e]) + gt_elem<DIM, double, true>(mk, A.vstar, e);
+                A.qtmp[e] = qv;
+                acc += qv * qv;
+            }
+            put_partial(acc, P0);
+            if (!grid_barrier(A.gb, &epoch)) return false;
+            rhs_scale = sqrt(all_sum(P0)) / A.scaleq;
+            if (!isfinite(rhs_scale)) {
+                o.status = GG_ERR_NONFINITE;
+                o.where = UZ_RHS;
+                return true;
+            }
+            // STEP 3 (:616-659): K u = f − G p
+            for (int64_t n = gtid(); n < nnode; n += gstride()) {
+                double g[DIM];
+                g_node<DIM, double, true>(mk, A.q, n, g);
+                const uint8_t bm = L0.bc[n];
+#pragma unroll
+                for (int c = 0; c < DIM; c++) {
+                    const int64_t i = (int64_t)c * nnode + n;
+                    A.ftmp[i] = A.f[i] - (((bm >> c) & 1) ? 0.0 : g[c]);
+                }
+            }
+            if (!grid_barrier(A.gb, &epoch)) return false;
+            stage = 2;
+            ib = A.ftmp;
+            ix = A.u;
+            irtol = A.inner_rtol;
+            continue;
+        }
+        if (stage == 2) {
+            // r = Gᵀu − h, and the exact-flow test: a velocity that meets the constraint
+            // to rounding ends the solve with the current pressure (no outer iteration)
+            double rr = 0.0, hh = 0.0, uu = 0.0;
+            for (int64_t e = gtid(); e < nel; e += gstride()) {
+                const double hvv = __ldcg(&A.hv[e]);
+                const double rv = -hvv + gt_elem<DIM, double, true>(mk, A.u, e);
+                A.r[e] = rv;
+                rr += rv * rv;
+                hh += hvv * hvv;
+            }
+            for (int64_t i = gtid(); i < (int64_t)DIM * nnode; i += gstride()) {
+                const double uv = __ldcg(&A.u[i]);
+                uu += uv * uv;
+            }
+            put_partial2(rr, hh, P0, P1);
+            put_partial(uu, P2);
+            if (!grid_barrier(A.gb, &epoch)) return false;
+            double r0, h2;
+            all_sum2(P0, P1, r0, h2);
+            r0 = sqrt(r0);
+            if (r0 <= A.floor_u * sqrt(all_sum(P2)) + A.floor_h * sqrt(h2)) {
+                exact = true;
+                absres = r0 / A.scaleq;
+                break;
+            }
+        } else {
+            // STEP 4 (:664-837), after K u* = G s: Gᵀu*, s·Gᵀu*, α
+            double acc = 0.0;
+            for (int64_t e = gtid(); e < nel; e += gstride()) {
+                const double qv = gt_elem<DIM, double, true>(mk, A.vstar, e);
+                A.qtmp[e] = qv;
+                acc += __ldcg(&A.s[e]) * qv;
+            }
+            put_partial(acc, P0);
+            if (!grid_barrier(A.gb, &epoch)) return false;
+            const double sq = all_sum(P0);
+            const double alpha = zr / sq;
+            if (!isfinite(zr) || !isfinite(sq) || !isfinite(alpha)) {
+                o.status = GG_ERR_NONFINITE;
+                o.where = UZ_STEP;
+                o.outer_iterations = it;
+                return true;
+            }
+            // p += α s, r −= α Gᵀu*, u −= α u*; ‖r‖
+            acc = 0.0;
+            for (int64_t e = gtid(); e < nel; e += gstride()) {
+                A.q[e] = alpha * __ldcg(&A.s[e]) + __ldcg(&A.q[e]);
+                const double rv = -alpha * __ldcg(&A.qtmp[e]) + __ldcg(&A.r[e]);
+                A.r[e] = rv;
+                acc += rv * rv;
+            }
+            for (int64_t i = gtid(); i < (int64_t)DIM * nnode; i += gstride())
+                A.u[i] = -alpha * __ldcg(&A.vstar[i]) + __ldcg(&A.u[i]);
+            put_partial(acc, P0);
+            if (!grid_barrier(A.gb, &epoch)) return false;
+            zr_prev = zr;
+            absres = sqrt(all_sum(P0)) / A.scaleq;
+            relres = absres / rhs_scale;
+            if (!isfinite(absres)) {
+                o.status = GG_ERR_NONFINITE;
+                o.where = UZ_RESIDUAL;
+                o.outer_iterations = it;
+                return true;
+            }
+            if (!(it < A.max_iterations)) {
+                it++;
+                o.status = GG_ERR_NOT_CONVERGED;
+                o.where = UZ_LIMIT;
+                break;
+            }
+            it++;
+            const double chosen = A.use_abs ? absres : relres;
+            if (!((chosen > A.tolerance) || (it < A.min_iterations))) break;
+        }
+        // the next conjugate direction: z = Ĝ⁻¹ r (or r), z·r
+        double acc = 0.0;
+        for (int64_t e = gtid(); e < nel; e += gstride()) {
+            const double rv = __ldcg(&A.r[e]);
+            const double z = A.use_precond ? rv / A.sdiag[e] : rv;
+            A.qtmp[e] = z;
+            acc += z * rv;
+        }
+        put_partial(acc, P0);
+        if (!grid_barrier(A.gb, &epoch)) return false;
+        zr = all_sum(P0);
+        const double beta = zr / zr_prev;
+        // s = z (first step) or z + β s
+        for (int64_t e = gtid(); e < nel; e += gstride()) {
+            const double z = __ldcg(&A.qtmp[e]);
+            A.s[e] = it == 0 ? z : z + beta * __ldcg(&A.s[e]);
+        }
+        if (!grid_barrier(A.gb, &epoch)) return false;
+        // G s, and the recycled start β u*_prev of K u* = G s
+        const bool warm = A.recycle && it > 0;
+        for (int64_t n = gtid(); n < nnode; n += gstride()) {
+            double g[DIM];
+            g_node<DIM, double, true>(mk, A.s, n, g);
+            const uint8_t bm = L0.bc[n];
+#pragma unroll
+            for (int c = 0; c < DIM; c++) {
+                const int64_t i = (int64_t)c * nnode + n;
+                A.ftmp[i] = ((bm >> c) & 1) ? 0.0 : g[c];
+                if (warm) A.vstar[i] = beta * __ldcg(&A.vstar[i]);
+            }
+        }
+        if (!grid_barrier(A.gb, &epoch)) return false;
+        stage = 3;
+        ib = A.ftmp;
+        ix = A.vstar;
+        irtol = A.inner_rtol;
+        iwarm = warm;
+    }
+    o.outer_iterations = it;
+    o.rel_residual = exact ? 0.0 : relres;
+    o.abs_residual = absres;
+    return true;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kFusedBlock, 2)
+k_uzawa_fused(const int4* __restrict__ tab, const UzawaFusedArgs A) {
+    __shared__ int4 s_tab[kTabWords];
+    for (int i = threadIdx.x; i < kTabWords; i += blockDim.x) s_tab[i] = tab[i];
+    __syncthreads();
+    const FusedTable& T = *reinterpret_cast<const FusedTable*>(s_tab);
+    UzawaFusedOut o;
+    // a barrier that gave up is reported by the barrier's own error word (read by the host)
+    if (uzawa_body<DIM>(T, A, o) && blockIdx.x == 0 && threadIdx.x == 0) *A.out = o;
 }
 
 // Algorithmic bytes of one iteration of the program: what each phase must read and write
@@ -739,11 +1137,6 @@ double program_bytes(const FusedTable& T, const std::vector<FusedPhase>& prog, i
     }
     return b;
 }
-
-struct FusedLaunch {
-    int max_blocks[4] = {0, 0, 0, 0};  // co-resident blocks per device, by DIM
-    bool probed[4] = {false, false, false, false};
-};
 
 }  // namespace
 
@@ -835,35 +1228,35 @@ bool fused_fcg_enabled() {
 // Multigrid FCG in one cooperative launch: x = K32⁻¹ b to ‖r‖ ≤ rtol‖b‖.  Returns
 // GG_OK / GG_ERR_NOT_CONVERGED / GG_ERR_NONFINITE / GG_ERR_CUDA, or 1 when the hierarchy
 // does not fit this kernel (the caller then runs the graph-captured solver).
-int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters) {
+// Co-resident blocks of the persistent kernel `fn` on this device (probed once per device
+// and kernel slot: DIM for k_fcg_fused, 4 + DIM for k_uzawa_fused; 0 where cooperative
+// launches are unavailable).
+static int fused_max_blocks(int slot, const void* fn) {
+    static std::mutex mu;
+    static int blocks[16][8];
+    static bool probed[16][8];
+    int dev = 0;
+    GG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16 || slot < 0 || slot >= 8) return 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!probed[dev][slot]) {
+        int coop = 0, per_sm = 0;
+        GG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        if (coop) GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kFusedBlock, 0));
+        blocks[dev][slot] = per_sm * num_sms();
+        probed[dev][slot] = true;
+    }
+    return blocks[dev][slot];
+}
+
+// The level table of the current hierarchy in device memory, for a flexible CG whose
+// solution is x and right-hand side b (level 0 smooths the FCG residual H.cgr32 into
+// H.z32).  Rebuilt when the hierarchy or those vectors change.  Returns 1 when the
+// hierarchy does not fit the persistent kernels.
+static int fused_table(Handle& H, const float* b, float* x) {
     const size_t nl = H.mg.size();
     const int deg = H.mg_degree;
     if (nl < 2 || nl > (size_t)kFusedMaxLevels || !H.coarse_n || deg < 2 || deg > 4) return 1;
-    const int dim = H.dim;
-    static std::mutex mu;
-    static FusedLaunch fl[16];
-    int dev = 0;
-    GG_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 16) return 1;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        FusedLaunch& f = fl[dev];
-        if (!f.probed[dim]) {
-            int coop = 0;
-            GG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-            int per_sm = 0;
-            if (coop) {
-                if (dim == 2)
-                    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fcg_fused<2>, kFusedBlock, 0));
-                else
-                    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fcg_fused<3>, kFusedBlock, 0));
-            }
-            f.max_blocks[dim] = per_sm * num_sms();
-            f.probed[dim] = true;
-        }
-        if (f.max_blocks[dim] <= 0) return 1;
-    }
-    const int max_blocks = fl[dev].max_blocks[dim];
     float* r = H.cgr32.as<float>();
     float* z = H.z32.as<float>();
     if (H.fused_gen != H.mg_gen || H.fused_r != r || H.fused_z != z || H.fused_x != x || H.fused_b != b) {
@@ -943,12 +1336,19 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
         H.fused_b = b;
         H.fused_phases = T.nphase;
     }
+    return GG_OK;
+}
+
+int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters) {
+    const int dim = H.dim;
+    const int max_blocks =
+        fused_max_blocks(dim, dim == 2 ? (const void*)k_fcg_fused<2> : (const void*)k_fcg_fused<3>);
+    if (max_blocks <= 0) return 1;
+    if (fused_table(H, b, x) != GG_OK) return 1;
     const int64_t n = H.ndof;
     const int64_t per = H.fused_dofs_per_block > 0 ? H.fused_dofs_per_block : kFusedBlock;
     int grid = (int)std::min<int64_t>((int64_t)max_blocks, (n + per - 1) / per);
     if (grid < 1) grid = 1;
-    // the barrier counter reaches (barriers of the launch) × grid: keep it inside 32 bits
-    if ((double)(maxit + 2) * (H.fused_phases + 1) * grid >= 2147483648.0) return 1;
     H.fused_part.ensure(sizeof(double) * 4 * grid);
     H.fused_bar.ensure(sizeof(GridBarrier));
     GG_CUDA(cudaMemsetAsync(H.fused_bar.p, 0, sizeof(GridBarrier), H.stream));
@@ -966,7 +1366,13 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
     GG_CUDA(cudaEventRecord(H.evf1, H.stream));
     H.kernel_launches += 1;
     GG_CUDA(cudaMemcpyAsync(H.h_scal, ks, sizeof(KrylovScalars), cudaMemcpyDeviceToHost, H.stream));
+    int* h_err = &H.h_scal[1].failed;  // pinned scratch word for the barrier's error flag
+    GG_CUDA(cudaMemcpyAsync(h_err, &gb->err, sizeof(int), cudaMemcpyDeviceToHost, H.stream));
     GG_CUDA(cudaStreamSynchronize(H.stream));
+    if (*h_err) {
+        H.err = "fused multigrid solve: grid barrier timed out";
+        return GG_ERR_CUDA;
+    }
     *iters = H.h_scal->iterations;
     {
         float ms = 0.f;
@@ -975,13 +1381,113 @@ int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, i
         H.fused_launches_acc++;
         H.fused_its_acc += H.h_scal->iterations;
     }
-    if (H.h_scal->failed == 4) {
-        H.err = "fused multigrid solve: grid barrier timed out";
-        return GG_ERR_CUDA;
-    }
     if (H.h_scal->failed == 1) return GG_ERR_NOT_CONVERGED;
     if (H.h_scal->failed) return GG_ERR_NONFINITE;
     return GG_OK;
+}
+
+// On unless the environment sets GALE_B200_FUSED_UZAWA=0, which selects the host-driven
+// Uzawa loop (read at every solve).
+bool fused_uzawa_enabled() {
+    const char* e = getenv("GALE_B200_FUSED_UZAWA");
+    return !(e && e[0] == '0');
+}
+
+int run_uzawa_fused(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
+    const int dim = H.dim;
+    const void* fn = dim == 2 ? (const void*)k_uzawa_fused<2> : (const void*)k_uzawa_fused<3>;
+    const int max_blocks = fused_max_blocks(4 + dim, fn);
+    if (max_blocks <= 0) return 1;
+    if (fused_table(H, H.r32.as<float>(), H.e32.as<float>()) != GG_OK) return 1;
+    const int64_t per = H.fused_dofs_per_block > 0 ? H.fused_dofs_per_block : kFusedBlock;
+    int grid = (int)std::min<int64_t>((int64_t)max_blocks, (H.ndof + per - 1) / per);
+    if (grid < 1) grid = 1;
+    H.fused_part.ensure(sizeof(double) * 8 * grid);
+    H.fused_bar.ensure(sizeof(GridBarrier));
+    H.fused_out.ensure(sizeof(UzawaFusedOut));
+    GG_CUDA(cudaMemsetAsync(H.fused_bar.p, 0, sizeof(GridBarrier), H.stream));
+    GG_CUDA(cudaMemsetAsync(H.fused_out.p, 0, sizeof(UzawaFusedOut), H.stream));
+    UzawaFusedArgs A;
+    std::memset(&A, 0, sizeof A);
+    A.mom64 = H.mom64.as<double>();
+    A.kdiag = H.kdiag64.as<double>();
+    A.sdiag = H.sdiag.as<double>();
+    A.f = H.f.as<double>();
+    A.hv = H.hvec.as<double>();
+    A.u = H.u.as<double>();
+    A.vstar = H.vstar.as<double>();
+    A.ftmp = H.ftmp.as<double>();
+    A.q = H.q.as<double>();
+    A.qtmp = H.qtmp.as<double>();
+    A.r = H.r.as<double>();
+    A.s = H.s.as<double>();
+    A.r64 = H.cg_r.as<double>();
+    A.e32 = H.e32.as<float>();
+    A.p32 = H.p32.as<float>();
+    A.Ap32 = H.Ap32.as<float>();
+    A.tolerance = prm.tolerance;
+    A.inner_rtol = prm.inner_rtol_factor * prm.tolerance;
+    A.scaleq = sqrt((double)H.nel);
+    double gmax = 0.0;
+    const int nen = 1 << dim;
+    for (int a = 0; a < nen; a++)
+        for (int c = 0; c < dim; c++) gmax = std::max(gmax, std::fabs(H.mk.Ge[a][c]));
+    A.floor_u = 64.0 * 2.220446049250313e-16 * gmax * std::sqrt((double)nen);
+    A.floor_h = 64.0 * 2.220446049250313e-16;
+    A.max_iterations = prm.max_iterations;
+    A.min_iterations = prm.min_iterations;
+    A.use_abs = prm.use_absolute_tolerance;
+    A.use_precond = prm.use_preconditioner;
+    A.recycle = prm.recycle_directions;
+    A.inner_maxit = prm.inner_max_iterations > 0 ? prm.inner_max_iterations : 10000;
+    A.sweep_cap = std::min(A.inner_maxit, 150);
+    A.out = H.fused_out.as<UzawaFusedOut>();
+    A.part = H.fused_part.as<double>();
+    A.gb = H.fused_bar.as<GridBarrier>();
+    const int4* tab = H.fused_tab.as<int4>();
+    void* args[] = {(void*)&tab, (void*)&A};
+    GG_CUDA(cudaEventRecord(H.evf0, H.stream));
+    GG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kFusedBlock), args, 0, H.stream));
+    GG_CUDA(cudaEventRecord(H.evf1, H.stream));
+    H.kernel_launches += 1;
+    UzawaFusedOut o;
+    GridBarrier gb;
+    GG_CUDA(cudaMemcpyAsync(&o, A.out, sizeof o, cudaMemcpyDeviceToHost, H.stream));
+    GG_CUDA(cudaMemcpyAsync(&gb, A.gb, sizeof gb, cudaMemcpyDeviceToHost, H.stream));
+    GG_CUDA(cudaStreamSynchronize(H.stream));
+    if (gb.err) {
+        H.err = "fused Uzawa solve: grid barrier timed out";
+        return GG_ERR_CUDA;
+    }
+    float ms = 0.f;
+    GG_CUDA(cudaEventElapsedTime(&ms, H.evf0, H.evf1));
+    S.outer_iterations = o.outer_iterations;
+    S.inner_iterations += o.inner_iterations;  // after any learned-correction calibration
+    S.inner_solves += o.inner_solves;
+    S.rel_residual = o.rel_residual;
+    S.abs_residual = o.abs_residual;
+    S.fused_launches = 1;
+    S.fused_iterations = o.inner_iterations;
+    S.fused_ms = ms;
+    S.fused_bytes_per_iteration = H.fused_bytes_it;
+    S.fused_barriers_per_iteration = H.fused_phases;
+    S.uzawa_fused = 1;
+    H.fail_where.clear();
+    static const char* kWhere[] = {"",
+                                   "first inner solve (K u* = f)",
+                                   "pressure right-hand side",
+                                   "velocity solve K u = f - G p",
+                                   "inner solve K u* = G s",
+                                   "conjugate-direction step",
+                                   "pressure residual",
+                                   "outer iteration limit reached"};
+    if (o.where > 0 && o.where < 8) {
+        H.fail_where = kWhere[o.where];
+        if (o.where != 7)
+            H.fail_where += " at outer iteration " + std::to_string(o.outer_iterations) + " (" +
+                            std::to_string(o.inner_iterations) + " inner iterations so far)";
+    }
+    return o.status;
 }
 
 }  // namespace gg

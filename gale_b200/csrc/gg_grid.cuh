@@ -24,7 +24,9 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
 }
 
 // All blocks of the grid meet here.  Arrival is a release reduction on a counter that only
-// grows (barrier e of the launch completes when it reaches e·gridDim.x); waiting is an
+// grows (barrier e of the launch completes when it reaches e·gridDim.x, modulo 2^32: the
+// counter runs at most gridDim.x ahead of or behind a waiting block's target, so the
+// signed difference decides and a launch may pass any number of barriers); waiting is an
 // acquire poll of that counter.  The release/acquire pair orders every write of the block
 // (made visible to thread 0 by __syncthreads) before every read after the barrier.
 // Returns false (uniformly within the block) once any block has given up waiting; the
@@ -38,7 +40,7 @@ __device__ __noinline__ bool grid_barrier(GridBarrier* gb, unsigned int* epoch,
         int ok = 1;
         asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&gb->arrive), "r"(1u) : "memory");
         long long spins = 0;
-        while (ld_acquire_gpu(&gb->arrive) < target) {
+        while ((int)(ld_acquire_gpu(&gb->arrive) - target) < 0) {
             if (++spins > spin_limit || ((spins & 1023) == 0 && *(volatile int*)&gb->err)) {
                 atomicExch(&gb->err, 1);
                 ok = 0;

@@ -116,7 +116,7 @@ struct Handle {
     int mg_degree = 2;      // Chebyshev degree of the smoother
     int build_shape[2] = {-1, -1};  // autotuned CTA shape of the FP64 / FP32 moment build
     // persistent multigrid FCG (gg_fused.cu): level table for the current hierarchy
-    DBuf fused_tab, fused_part, fused_bar;
+    DBuf fused_tab, fused_part, fused_bar, fused_out;
     std::vector<unsigned char> fused_host;
     int64_t fused_gen = -2;  // mg_gen the table was written for
     const float* fused_r = nullptr;  // FCG residual / preconditioned vector baked into it

@@ -88,6 +88,11 @@ int fcg_mg_solve(Handle& H, const float* b, float* x, double rtol, int maxit, in
 // hierarchy does not fit it (no dense coarse level, > 8 levels, degree outside 2..4).
 int run_fcg_fused(Handle& H, const float* b, float* x, double rtol, int maxit, int* iters);
 bool fused_fcg_enabled();
+// The mixed-path Uzawa solve (multigrid inner solves) as one cooperative launch; 1 when it
+// does not apply (the caller runs the host-driven loop), else the solve's status with S's
+// iteration counts, residuals and launch figures filled and H.fail_where set on failure.
+int run_uzawa_fused(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S);
+bool fused_uzawa_enabled();
 // µs per grid barrier of the persistent kernels (measurement, gg_fused.cu)
 int time_grid_barrier(int blocks_per_sm, int iters, double* us);
 // the grid barrier's give-up path with a short limit (block 0 never arrives)

@@ -109,27 +109,14 @@ int apply_grid(int64_t nel) {
 }
 
 // ---- G p (P0 pressure → velocity force): node-centric gather, BC rows zero ----------
-// G_e[a][c] = Σ_gauss w (−detJ) ∂N_a/∂x_c (GradientStiffnessMatrixTerm.cxx:213-246).
 template <int DIM, typename R>
 __global__ void k_apply_G(MeshK mk, const uint8_t* __restrict__ bcmask, const R* __restrict__ p,
                           R* __restrict__ y, R beta) {
     const int64_t nnode = mk.nnode;
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nnode;
          n += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(n % mk.nn[0]);
-        const int j = (int)((n / mk.nn[0]) % mk.nn[1]);
-        const int k = DIM == 3 ? (int)(n / ((int64_t)mk.nn[0] * mk.nn[1])) : 0;
         R acc[DIM];
-#pragma unroll
-        for (int c = 0; c < DIM; c++) acc[c] = R(0);
-#pragma unroll
-        for (int a = 0; a < (1 << DIM); a++) {
-            const int ei = i - (a & 1), ej = j - ((a >> 1) & 1), ek = DIM == 3 ? k - ((a >> 2) & 1) : 0;
-            if (ei < 0 || ej < 0 || ek < 0 || ei >= mk.n[0] || ej >= mk.n[1] || ek >= mk.n[2]) continue;
-            const R pv = p[ei + (int64_t)mk.n[0] * (ej + (int64_t)mk.n[1] * ek)];
-#pragma unroll
-            for (int c = 0; c < DIM; c++) acc[c] += (R)mk.Ge[a][c] * pv;
-        }
+        g_node<DIM, R, false>(mk, p, n, acc);
         const uint8_t bm = bcmask[n];
 #pragma unroll
         for (int c = 0; c < DIM; c++) {
@@ -142,20 +129,10 @@ __global__ void k_apply_G(MeshK mk, const uint8_t* __restrict__ bcmask, const R*
 // ---- Gᵀ u (velocity → element): element-centric, all columns --------------------------
 template <int DIM, typename R>
 __global__ void k_apply_GT(MeshK mk, const R* __restrict__ u, R* __restrict__ q) {
-    const int64_t nel = mk.nel, nnode = mk.nnode;
+    const int64_t nel = mk.nel;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        int ijk[3];
-        elem_ijk(mk, e, ijk);
-        R s = R(0);
-#pragma unroll
-        for (int a = 0; a < (1 << DIM); a++) {
-            const int64_t n = elem_node<DIM>(mk, ijk, a);
-#pragma unroll
-            for (int c = 0; c < DIM; c++) s += (R)mk.Ge[a][c] * u[(int64_t)c * nnode + n];
-        }
-        q[e] = s;
-    }
+         e += (int64_t)gridDim.x * blockDim.x)
+        q[e] = gt_elem<DIM, R, false>(mk, u, e);
 }
 
 void apply_G(const Handle& H, const double* p, double* y, cudaStream_t st) {

@@ -247,6 +247,49 @@ __device__ __forceinline__ void apply_split(const MeshK& mk, const R* __restrict
     }
 }
 
+// (G p) at node n, component by component, before the BC rows are zeroed: the gather of
+// the 2^dim elements around the node in element-corner order a = 0 … 2^dim−1,
+// G_e[a][c] = Σ_gauss w (−detJ) ∂N_a/∂x_c (GradientStiffnessMatrixTerm.cxx:213-246).
+// kCoherent reads p through L2 only (p written earlier in the same launch).
+template <int DIM, typename R, bool kCoherent>
+__device__ __forceinline__ void g_node(const MeshK& mk, const R* __restrict__ p, int64_t n, R (&acc)[DIM]) {
+    const int i = (int)(n % mk.nn[0]);
+    const int j = (int)((n / mk.nn[0]) % mk.nn[1]);
+    const int k = DIM == 3 ? (int)(n / ((int64_t)mk.nn[0] * mk.nn[1])) : 0;
+#pragma unroll
+    for (int c = 0; c < DIM; c++) acc[c] = R(0);
+#pragma unroll
+    for (int a = 0; a < (1 << DIM); a++) {
+        const int ei = i - (a & 1), ej = j - ((a >> 1) & 1), ek = DIM == 3 ? k - ((a >> 2) & 1) : 0;
+        if (ei < 0 || ej < 0 || ek < 0 || ei >= mk.n[0] || ej >= mk.n[1] || ek >= mk.n[2]) continue;
+        const R* pe = &p[ei + (int64_t)mk.n[0] * (ej + (int64_t)mk.n[1] * ek)];
+        const R pv = kCoherent ? __ldcg(pe) : *pe;
+#pragma unroll
+        for (int c = 0; c < DIM; c++) acc[c] += (R)mk.Ge[a][c] * pv;
+    }
+}
+
+// (Gᵀ u) of element e: Σ over corners a and components c of G_e[a][c] u_{a,c}
+template <int DIM, typename R, bool kCoherent>
+__device__ __forceinline__ R gt_elem(const MeshK& mk, const R* __restrict__ u, int64_t e) {
+    const int64_t nnode = mk.nnode;
+    const int i0 = (int)(e % mk.n[0]);
+    const int64_t rr = e / mk.n[0];
+    const int j0 = (int)(rr % mk.n[1]), k0 = DIM == 3 ? (int)(rr / mk.n[1]) : 0;
+    R s = R(0);
+#pragma unroll
+    for (int a = 0; a < (1 << DIM); a++) {
+        const int64_t n = (i0 + (a & 1)) + (int64_t)mk.nn[0] * ((j0 + ((a >> 1) & 1)) +
+                                                            (int64_t)mk.nn[1] * (DIM == 3 ? k0 + ((a >> 2) & 1) : 0));
+#pragma unroll
+        for (int c = 0; c < DIM; c++) {
+            const R* up = &u[(int64_t)c * nnode + n];
+            s += (R)mk.Ge[a][c] * (kCoherent ? __ldcg(up) : *up);
+        }
+    }
+    return s;
+}
+
 // The FP64 apply is summed in a fixed order: elements are split into the 2^dim parity
 // classes color = (i&1) | (j&1)<<1 | (k&1)<<2, and one launch scatters one class.  Two
 // elements of the same class share no node, so every atomic of a launch lands on a node

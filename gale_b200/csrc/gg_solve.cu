@@ -832,84 +832,110 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
         }
         H.nn_verdict = H.nn_enabled ? 1 : 0;
     }
-    // STEP 1 (:553-565)
-    if ((rc = inner(f, vstar, prm.tolerance)) != GG_OK) return fail("first inner solve (K u* = f)", rc);
-    apply_GT(H, vstar, qtmp, st);
-    H.kernel_launches++;
-    axpby(H, ne, -1.0, hv, 1.0, qtmp);
-    const double inner_rtol = prm.inner_rtol_factor * prm.tolerance;
-    const double rhs_scale = sqrt(dot(H, ne, qtmp, qtmp)) / scaleq;
-    if (!isfinite(rhs_scale)) return GG_ERR_NONFINITE;
-    // STEP 3 (:616-659)
-    apply_G(H, q, ftmp, st);
-    H.kernel_launches++;
-    axpby(H, nd, 1.0, f, -1.0, ftmp);
-    if ((rc = inner(ftmp, u, inner_rtol)) != GG_OK) return fail("velocity solve K u = f - G p", rc);
-    apply_GT(H, u, r, st);
-    H.kernel_launches++;
-    axpby(H, ne, -1.0, hv, 1.0, r);
-    // STEP 4 (:664-837)
-    double zr_prev = 1.0, absres = 0.0, relres = 0.0;
+    double absres = 0.0, relres = 0.0;
     bool exact = false;
-    {
-        // A velocity that already meets the constraint to rounding (boundary velocities
-        // that admit an exactly representable flow, found by the inner solve): r0 is then
-        // rounding noise whose constant-pressure part the Schur CG cannot remove, and the
-        // reference's loop would iterate on noise until α breaks down.  The solve ends at
-        // once with the current pressure (no outer iteration, relative residual 0).
-        double gmax = 0.0;
-        const int nen = 1 << H.dim;
-        for (int a = 0; a < nen; a++)
-            for (int c = 0; c < H.dim; c++) gmax = std::max(gmax, std::fabs(H.mk.Ge[a][c]));
-        const double floor_r = 64.0 * 2.220446049250313e-16 *
-                               (gmax * std::sqrt((double)nen) * std::sqrt(dot(H, nd, u, u)) + std::sqrt(dot(H, ne, hv, hv)));
-        const double r0 = std::sqrt(dot(H, ne, r, r));
-        if (r0 <= floor_r) {
-            exact = true;
-            absres = r0 / scaleq;
-        }
+    // the whole solve in one persistent launch where it applies: mixed precision with
+    // multigrid inner solves (the learned variant when its correction is off)
+    const bool mg_inner = prm.inner == GG_INNER_MG_CG ||
+                          (prm.inner == GG_INNER_LEARNED_CG && !(learned_usable(H, prm) && H.nn_enabled));
+    int fused_rc = 1;
+    if (mixed && mg_inner && fused_fcg_enabled() && fused_uzawa_enabled()) {
+        if ((rc = mg_setup(H)) != GG_OK) return rc;
+        fused_rc = run_uzawa_fused(H, prm, S);
     }
-    while (!exact) {
-        if (prm.use_preconditioner) {
-            k_div<<<grid_for(ne, 256), 256, 0, st>>>(ne, r, H.sdiag.as<double>(), qtmp);
-            H.kernel_launches++;
-        } else {
-            GG_CUDA(cudaMemcpyAsync(qtmp, r, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
+    if (fused_rc != 1) {
+        rc = fused_rc;
+        it = S.outer_iterations;
+        absres = S.abs_residual;
+        relres = S.rel_residual;
+        H.fused_launches_acc = S.fused_launches;
+        H.fused_its_acc = S.fused_iterations;
+        H.fused_ms_acc = S.fused_ms;
+        // a step that failed ends the solve at once (as fail() below); the iteration limit
+        // reports the residuals reached
+        if (rc != GG_OK && !(rc == GG_ERR_NOT_CONVERGED && H.fail_where == "outer iteration limit reached")) {
+            S.fallbacks = H.fallbacks;
+            return rc;
         }
-        const double zr = dot(H, ne, qtmp, r);
-        if (it == 0)
-            GG_CUDA(cudaMemcpyAsync(s, qtmp, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
-        else
-            axpby(H, ne, 1.0, qtmp, zr / zr_prev, s);
-        apply_G(H, s, ftmp, st);
-        H.kernel_launches++;
-        // recycling (fast path only): s = z + β s_prev, so β u*_prev = K⁻¹ G (β s_prev)
-        // is a start for K u* = G s that leaves only K⁻¹ G z to find; the stopping rule
-        // stays relative to ‖G s‖
-        const bool warm = prm.recycle_directions && prm.precision == GG_PRECISION_MIXED && it > 0;
-        if (warm) axpby(H, nd, 0.0, vstar, zr / zr_prev, vstar);
-        if ((rc = inner(ftmp, vstar, inner_rtol, warm)) != GG_OK) return fail("inner solve K u* = G s", rc);
+    } else {
+        // STEP 1 (:553-565)
+        if ((rc = inner(f, vstar, prm.tolerance)) != GG_OK) return fail("first inner solve (K u* = f)", rc);
         apply_GT(H, vstar, qtmp, st);
         H.kernel_launches++;
-        const double sq = dot(H, ne, s, qtmp);
-        const double alpha = zr / sq;
-        if (!isfinite(zr) || !isfinite(sq) || !isfinite(alpha)) return fail("conjugate-direction step", GG_ERR_NONFINITE);
-        axpby(H, ne, alpha, s, 1.0, q);
-        axpby(H, nd, -alpha, vstar, 1.0, u);
-        axpby(H, ne, -alpha, qtmp, 1.0, r);
-        zr_prev = zr;
-        absres = sqrt(dot(H, ne, r, r)) / scaleq;
-        relres = absres / rhs_scale;
-        if (!isfinite(absres)) return fail("pressure residual", GG_ERR_NONFINITE);
-        if (!(it < prm.max_iterations)) {
-            rc = GG_ERR_NOT_CONVERGED;
-            it++;
-            H.fail_where = "outer iteration limit reached";
-            break;
+        axpby(H, ne, -1.0, hv, 1.0, qtmp);
+        const double inner_rtol = prm.inner_rtol_factor * prm.tolerance;
+        const double rhs_scale = sqrt(dot(H, ne, qtmp, qtmp)) / scaleq;
+        if (!isfinite(rhs_scale)) return GG_ERR_NONFINITE;
+        // STEP 3 (:616-659)
+        apply_G(H, q, ftmp, st);
+        H.kernel_launches++;
+        axpby(H, nd, 1.0, f, -1.0, ftmp);
+        if ((rc = inner(ftmp, u, inner_rtol)) != GG_OK) return fail("velocity solve K u = f - G p", rc);
+        apply_GT(H, u, r, st);
+        H.kernel_launches++;
+        axpby(H, ne, -1.0, hv, 1.0, r);
+        // STEP 4 (:664-837)
+        double zr_prev = 1.0;
+        {
+            // A velocity that already meets the constraint to rounding (boundary velocities
+            // that admit an exactly representable flow, found by the inner solve): r0 is then
+            // rounding noise whose constant-pressure part the Schur CG cannot remove, and the
+            // reference's loop would iterate on noise until α breaks down.  The solve ends at
+            // once with the current pressure (no outer iteration, relative residual 0).
+            double gmax = 0.0;
+            const int nen = 1 << H.dim;
+            for (int a = 0; a < nen; a++)
+                for (int c = 0; c < H.dim; c++) gmax = std::max(gmax, std::fabs(H.mk.Ge[a][c]));
+            const double floor_r = 64.0 * 2.220446049250313e-16 *
+                                   (gmax * std::sqrt((double)nen) * std::sqrt(dot(H, nd, u, u)) + std::sqrt(dot(H, ne, hv, hv)));
+            const double r0 = std::sqrt(dot(H, ne, r, r));
+            if (r0 <= floor_r) {
+                exact = true;
+                absres = r0 / scaleq;
+            }
         }
-        it++;
-        const double chosen = prm.use_absolute_tolerance ? absres : relres;
-        if (!((chosen > prm.tolerance) || (it < prm.min_iterations))) break;
+        while (!exact) {
+            if (prm.use_preconditioner) {
+                k_div<<<grid_for(ne, 256), 256, 0, st>>>(ne, r, H.sdiag.as<double>(), qtmp);
+                H.kernel_launches++;
+            } else {
+                GG_CUDA(cudaMemcpyAsync(qtmp, r, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
+            }
+            const double zr = dot(H, ne, qtmp, r);
+            if (it == 0)
+                GG_CUDA(cudaMemcpyAsync(s, qtmp, sizeof(double) * ne, cudaMemcpyDeviceToDevice, st));
+            else
+                axpby(H, ne, 1.0, qtmp, zr / zr_prev, s);
+            apply_G(H, s, ftmp, st);
+            H.kernel_launches++;
+            // recycling (fast path only): s = z + β s_prev, so β u*_prev = K⁻¹ G (β s_prev)
+            // is a start for K u* = G s that leaves only K⁻¹ G z to find; the stopping rule
+            // stays relative to ‖G s‖
+            const bool warm = prm.recycle_directions && prm.precision == GG_PRECISION_MIXED && it > 0;
+            if (warm) axpby(H, nd, 0.0, vstar, zr / zr_prev, vstar);
+            if ((rc = inner(ftmp, vstar, inner_rtol, warm)) != GG_OK) return fail("inner solve K u* = G s", rc);
+            apply_GT(H, vstar, qtmp, st);
+            H.kernel_launches++;
+            const double sq = dot(H, ne, s, qtmp);
+            const double alpha = zr / sq;
+            if (!isfinite(zr) || !isfinite(sq) || !isfinite(alpha)) return fail("conjugate-direction step", GG_ERR_NONFINITE);
+            axpby(H, ne, alpha, s, 1.0, q);
+            axpby(H, nd, -alpha, vstar, 1.0, u);
+            axpby(H, ne, -alpha, qtmp, 1.0, r);
+            zr_prev = zr;
+            absres = sqrt(dot(H, ne, r, r)) / scaleq;
+            relres = absres / rhs_scale;
+            if (!isfinite(absres)) return fail("pressure residual", GG_ERR_NONFINITE);
+            if (!(it < prm.max_iterations)) {
+                rc = GG_ERR_NOT_CONVERGED;
+                it++;
+                H.fail_where = "outer iteration limit reached";
+                break;
+            }
+            it++;
+            const double chosen = prm.use_absolute_tolerance ? absres : relres;
+            if (!((chosen > prm.tolerance) || (it < prm.min_iterations))) break;
+        }
     }
     if (exact) relres = 0.0;
     S.outer_iterations = it;
@@ -919,6 +945,7 @@ int uzawa_solve(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     S.fused_ms = H.fused_ms_acc;
     S.fused_bytes_per_iteration = H.fused_launches_acc ? H.fused_bytes_it : 0.0;
     S.fused_barriers_per_iteration = H.fused_launches_acc ? H.fused_phases : 0;
+    S.uzawa_fused = fused_rc != 1 ? 1 : 0;
     // the first solve after a build also accounts for the build's kernels
     S.kernel_launches = H.kernel_launches - (H.stats_gen != H.build_gen ? H.launches_at_build : launches0);
     H.stats_gen = H.build_gen;

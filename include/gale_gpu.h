@@ -191,7 +191,9 @@ typedef struct gg_uzawa_stats {
     double  fused_ms;
     double  fused_bytes_per_iteration;
     int32_t fused_barriers_per_iteration;
-    int32_t pad_stats;
+    int32_t uzawa_fused;          /* 1: the whole solve ran as one persistent launch (mixed
+                                     path, multigrid inner solves): fused_launches is then 1,
+                                     fused_ms that launch's device time                   */
 } gg_uzawa_stats;
 
 typedef struct gg_picard_params {
