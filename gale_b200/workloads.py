@@ -137,6 +137,30 @@ def creep_3d(n=64, ppc=27, seed=2024, noise=0.05, theta=9.21, rayleigh=1e6, tole
                     meta={"n": n, "ppc": ppc, "seed": seed})
 
 
+def velic_solcx(n=64, ppc=20, eta_a=100.0, eta_b=1.0, xc=0.5, nz=2, nx=1, tolerance=1e-5) -> Workload:
+    """Underworld's Velic solCx benchmark (testVelicSolCx.xml, Analytic plugin
+    Underworld/SysTest/AnalyticPlugins/Velic_solCx): unit square, free-slip walls, a viscosity
+    step at x = xc (η_A = 100 left, η_B = 1 right, two MaterialViscosity materials assigned
+    by point position), driven by the thermal buoyancy f_y = Ra·T with Ra = 1 and the nodal
+    temperature T = sin(n_z π y) cos(n_x π x) (StandardConditionFunctions' VelicTemperatureIC,
+    wavenumberY = 2, wavenumberX = 1).  Points and weights as the deck's PIC components
+    (PICellerator/Apps/PIC_Components/MaterialPointSwarm.xml): SpaceFillerParticleLayout
+    with 20 points per element, PCDVC weights at resolution 10 (lowerT 0.6, upperT 25,
+    3 splits, 3 deletions)."""
+    mesh = Mesh(2, (n, n), (0.0, 0.0), (1.0, 1.0))
+    from .layouts import space_filler
+    coords = space_filler(mesh, ppc)
+    material = (coords[:, 0] >= xc).astype(np.int32)
+    nodes = node_coords(mesh)
+    T = np.sin(nz * np.pi * nodes[:, 1]) * np.cos(nx * np.pi * nodes[:, 0])
+    mats = [RheologyMaterial([MaterialViscosity(eta_a)]), RheologyMaterial([MaterialViscosity(eta_b)])]
+    return Workload("velic_solcx", mesh, free_slip(2), mats, BodyForce(rayleighNumber=1.0), coords, material,
+                    temperature=np.ascontiguousarray(T), uzawa=UzawaSolver(tolerance=tolerance),
+                    meta={"n": n, "ppc": ppc, "eta_a": eta_a, "eta_b": eta_b, "xc": xc, "nz": nz, "nx": nx,
+                          "weights_resolution": 10,
+                          "pcdvc": dict(upperT=25.0, lowerT=0.6, maxSplits=3, maxDeletions=3)})
+
+
 def extension_2d(nx=256, ny=64, ppc=40, seed=7, width=4.0, picard_its=20, tolerance=1e-5) -> Workload:
     """2D viscoplastic extension on [0,4]×[0,1] (domain assumed: square elements).
     Layers: mantle y<0.5 (η=1), lower crust 0.5≤y<0.75 (η=1e2), upper crust y≥0.75
