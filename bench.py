@@ -183,6 +183,10 @@ def gale_arm(args):
     if args.inner == "learned":
         mg = UzawaSolver(tolerance=1e-6, precision="mixed", inner="mg", smoothingDegree=args.smoothing_degree)
         t_mg, st_mg, _ = timed(mg, "mixed", max(1, args.steps // 2), 1)
+    # the same Jacobi-preconditioned CG as the plain path, in FP32 sweeps inside FP64 defect
+    # correction: what the precision alone buys, apart from multigrid
+    mj = UzawaSolver(tolerance=1e-6, precision="mixed", inner="jacobi")
+    t_mj, st_mj, _ = timed(mj, "mixed", max(1, args.steps // 2), 1)
     accuracy = None
     if not args.no_accuracy:
         deep = dict(innerRtolFactor=0.01, innerMaxIterations=400000, maxIterations=5000)
@@ -347,6 +351,7 @@ def gale_arm(args):
                        "parallelism": f"replicas x{world}"},
             "plain_fp64_s": t_plain, "speedup_vs_plain_fp64": t_plain / t_head,
             "multigrid_without_learned_s": t_mg,
+            "mixed_jacobi_s": t_mj,
             "solves_per_s": world / t_head,
             "rel_l2_vs_fp64": {"u": err_u, "p": err_p},
             "accuracy": accuracy,
@@ -357,6 +362,7 @@ def gale_arm(args):
             "iterations": {"headline": {k: st_head[k] for k in ("outer_iterations", "inner_iterations")},
                            "multigrid_without_learned": None if st_mg is None else
                            {k: st_mg[k] for k in ("outer_iterations", "inner_iterations")},
+                           "mixed_jacobi": {k: st_mj[k] for k in ("outer_iterations", "inner_iterations")},
                            "plain_fp64": {k: st_plain[k] for k in ("outer_iterations", "inner_iterations")}},
             "gpu_launches": int(st_head["kernel_launches"]) * args.steps,
             "roofline": {"bound": "hbm",
