@@ -5,16 +5,19 @@
 // about a hundred kernels per iteration, and on the coarse levels each does a few
 // microseconds of work, so kernel boundaries set the pace.  Here one cooperative launch
 // runs a whole FP32 solve.  The phases of an iteration are:
-//   fine apply → update → (V-cycle: smoothing, restriction, dense coarse solve,
-//   prolongation on every level) → dot products → direction
+//   V-cycle (smoothing, restriction, dense coarse solve, prolongation on every level, the
+//   dot products fused into the last smoothing step) → fine apply of the direction →
+//   update (+ the next level-0 Chebyshev start)
 // Each phase boundary is a grid barrier instead of a kernel boundary.  The host writes the
 // phase list of one iteration (a "program" for the level hierarchy at hand) into a table
 // in device memory; the kernel copies it to shared memory and runs it with one switch, so
-// each phase body, the element apply above all, is compiled once.  Neighbouring node-wise
-// phases are fused:
+// each phase body, the element apply above all, is compiled once.  Neighbouring phases
+// are fused:
 //   * the update with the level-0 Chebyshev start;
-//   * the last smoothing step with the FCG dot products;
-//   * the restriction with the coarse Chebyshev start.
+//   * the last smoothing step with the FCG dot products (and the zeroing of Ap);
+//   * the restriction with the coarse Chebyshev start;
+//   * the direction p = z + βp with the apply of it (formed at the element gather) and
+//     with the update (which stores it), so it has no phase of its own.
 // The per-phase arithmetic is that of the separate kernels, so the iterates are those of
 // run_fcg up to the order of FP32 atomic sums.
 //
@@ -77,9 +80,8 @@ enum : uint8_t {
     PH_DENSE = 4,      // x_l = A_l⁻¹ b_l (coarsest level)
     PH_PROLONG = 5,    // x_l += P x_{l+1}, t_l = 0
     PH_RESTART = 6,    // post-smoothing start on level l
-    PH_DIR = 7,        // FCG: p = z + βp, Ap = 0
-    PH_APPLY_P = 8,    // FCG: Ap = K p with the partials of pᵀAp
-    PH_UPDATE = 9,     // FCG: x += αp, r −= αAp, ‖r‖² partials, level-0 Chebyshev start
+    PH_APPLY_P = 8,    // FCG: Ap = K p for p = z + βp formed at the gather, partials of pᵀAp
+    PH_UPDATE = 9,     // FCG: p = z + βp, x += αp, r −= αAp, ‖r‖² partials, level-0 start
 };
 
 struct FusedPhase {
@@ -181,13 +183,16 @@ __device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * block
 // (kEnergy is only asked on level 0).  Measured per phase on creep 64³: the 16³ and 8³
 // applies 4.4 → 3.7 and 4.3 → 3.1 µs; the 32³ level (1.3 items per thread) was slower
 // split, 5.0 → 5.6 µs.
-template <int DIM, bool kEnergy>
-__device__ __forceinline__ double phase_apply(const FusedLevel& L, const float* v, float* t) {
-    if (!kEnergy && (int64_t)DIM * L.mk.nel <= gstride()) {
+// kAxpy: the applied vector is v + beta·v2, formed at the element gather.
+template <int DIM, bool kEnergy, bool kAxpy = false>
+__device__ __forceinline__ double phase_apply(const FusedLevel& L, const float* v, float* t,
+                                              const float* v2 = nullptr, float beta = 0.f) {
+    if (!kEnergy && !kAxpy && (int64_t)DIM * L.mk.nel <= gstride()) {
         apply_split<DIM, float, 1>(L.mk, L.mom, L.bc, v, t, gtid(), gstride());
         return 0.0;
     }
-    return apply_tiles<DIM, float, 1, kEnergy>(L.mk, L.mom, L.bc, v, t, blockIdx.x, gridDim.x);
+    return apply_tiles<DIM, float, 1, kEnergy, ApplyTile<DIM>::Y, ApplyTile<DIM>::Z, kAxpy>(
+        L.mk, L.mom, L.bc, v, t, blockIdx.x, gridDim.x, v2, beta);
 }
 
 // Node-wise phases work on slices of W consecutive FP32 elements: W = 4 moves slice v
@@ -266,9 +271,10 @@ __device__ __forceinline__ void phase_cheb_step(const FusedLevel& L, int k, bool
     });
 }
 
-// the same step on level 0, finishing z, with the FCG partial sums r·z and z·Ap
+// the same step on level 0, finishing z, with the FCG partial sums r·z and z·Ap; Ap is
+// zeroed once read (the direction's apply accumulates into it)
 template <int DIM>
-__device__ __forceinline__ void phase_cheb_step_dots(const FusedLevel& L, int k, const float* Ap, double& rz,
+__device__ __forceinline__ void phase_cheb_step_dots(const FusedLevel& L, int k, float* Ap, double& rz,
                                                      double& zap, bool vec) {
     const float c1 = L.c1[k], c2 = L.c2[k];
     for_slices((int64_t)DIM * L.mk.nnode, vec, [&](auto w, int64_t v) {
@@ -294,6 +300,7 @@ __device__ __forceinline__ void phase_cheb_step_dots(const FusedLevel& L, int k,
         st<W>(L.d, v, d);
         st<W>(L.x, v, z);
         st<W>(L.t, v, z0);
+        st<W>(Ap, v, z0);
     });
 }
 
@@ -499,11 +506,13 @@ __device__ __forceinline__ void phase_dense(int n, const float* A, const float* 
     }
 }
 
-// x = 0, r = b (BC rows zero), p = Ap = 0 (update = false); or x += αp, r −= αAp
-// (update = true); then the level-0 Chebyshev start on r.  Returns this thread's Σ r².
+// x = 0, r = b (BC rows zero), p = Ap = 0 (update = false); or p = z + βp, x += αp,
+// r −= αAp (update = true); then the level-0 Chebyshev start on r.  Returns this
+// thread's Σ r².
 template <int DIM>
-__device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool update, float alpha, const float* b,
-                                                     const double* b64, float* x, float* p, float* Ap, bool vec) {
+__device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool update, float alpha, float beta,
+                                                     const float* b, const double* b64, float* x, float* p,
+                                                     float* Ap, bool vec) {
     const int64_t nnode = L0.mk.nnode, n = (int64_t)DIM * nnode;
     float* r = L0.b;
     float* z = L0.x;
@@ -512,14 +521,16 @@ __device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool 
         const float th = L0.inv_theta;
         for_slices(n, vec, [&](auto w, int64_t v) {
             constexpr int W = decltype(w)::value;
-            float xv[W], pv[W], rv[W], ap[W], iv[W], d[W], z0[W];
+            float xv[W], pv[W], rv[W], ap[W], iv[W], d[W], z0[W], zv[W];
             ld_cg<W>(x, v, xv);
             ld_cg<W>(p, v, pv);
             ld_cg<W>(r, v, rv);
             ld_cg<W>(Ap, v, ap);
             ld_ro<W>(L0.invd, v, iv);
+            ld_cg<W>(z, v, zv);
 #pragma unroll
             for (int e = 0; e < W; e++) {
+                pv[e] = zv[e] + beta * pv[e];  // the direction the apply formed: p = z + βp
                 xv[e] = xv[e] + alpha * pv[e];
                 rv[e] = rv[e] - alpha * ap[e];  // BC rows of Ap are zero
                 acc += (double)rv[e] * (double)rv[e];
@@ -527,6 +538,7 @@ __device__ __forceinline__ double phase_update_start(const FusedLevel& L0, bool 
                 z0[e] = 0.f;
             }
             st<W>(x, v, xv);
+            st<W>(p, v, pv);
             st<W>(r, v, rv);
             st<W>(L0.r, v, rv);
             st<W>(L0.d, v, d);
@@ -581,7 +593,7 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, co
     double* p_zap = part + 2 * G;
     double* p_pap = part + 3 * G;
     const bool vec = T.vec4 != 0;
-    put_partial(phase_update_start<DIM>(L0, false, 0.f, b, b64, x, p, Ap, vec), p_rr);
+    put_partial(phase_update_start<DIM>(L0, false, 0.f, 0.f, b, b64, x, p, Ap, vec), p_rr);
     if (!grid_barrier(gb, &epoch)) return false;
     const double rnorm0 = sqrt(all_sum(p_rr));
     const double tt = rtol * rnorm0;
@@ -598,8 +610,8 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, co
                 case PH_APPLY:
                     phase_apply<DIM, false>(L, P.flag ? L.x : L.d, L.t);
                     break;
-                case PH_APPLY_P:
-                    put_partial(phase_apply<DIM, true>(L0, p, Ap), p_pap);
+                case PH_APPLY_P:  // Ap = K(z + βp), with the partials of pᵀAp
+                    put_partial(phase_apply<DIM, true, true>(L0, L0.x, Ap, p, beta), p_pap);
                     break;
                 case PH_STEP:
                     phase_cheb_step<DIM>(L, P.k, vec);
@@ -627,23 +639,8 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, co
                 case PH_RESTART:
                     phase_restart<DIM>(L, vec);
                     break;
-                case PH_DIR:
-                    for_slices(n, vec, [&](auto w, int64_t v) {
-                        constexpr int W = decltype(w)::value;
-                        float zv[W], pv[W], z0[W];
-                        ld_cg<W>(L0.x, v, zv);
-                        ld_cg<W>(p, v, pv);
-#pragma unroll
-                        for (int e = 0; e < W; e++) {
-                            pv[e] = zv[e] + beta * pv[e];
-                            z0[e] = 0.f;
-                        }
-                        st<W>(p, v, pv);
-                        st<W>(Ap, v, z0);
-                    });
-                    break;
                 case PH_UPDATE:
-                    put_partial(phase_update_start<DIM>(L0, true, alpha, b, b64, x, p, Ap, vec), p_rr);
+                    put_partial(phase_update_start<DIM>(L0, true, alpha, beta, b, b64, x, p, Ap, vec), p_rr);
                     break;
                 default:
                     break;
@@ -764,18 +761,31 @@ struct UzawaFusedArgs {
     GridBarrier* gb;
 };
 
-// r64 = K x (r64 zero on entry): one phase per element parity class, so every node sums
-// its element terms in class order.  False if a barrier gave up.
+// The FP64 apply of the defect: true sums every node's element terms in parity-class order
+// (one phase per class, the same bits on every run); false scatters all elements in one
+// phase with FP64 atomics (arrival order).  The mixed path's iterates already depend on the
+// FP32 atomics' order, so it takes the one-phase apply: measured on creep 64³ (136 outer
+// iterations, 692 flexible-CG iterations), the solve's FP64 applies cost 30.6 ms in class
+// order and 11.5 ms in one phase.
+constexpr bool kUzClassOrderedK64 = false;
+
+// r64 = K x (r64 zero on entry).  False if a barrier gave up.
 template <int DIM>
 __device__ __forceinline__ bool uz_apply_K64(const FusedTable& T, const UzawaFusedArgs& A, const double* x,
                                              unsigned int& epoch) {
     const FusedLevel& L0 = T.lv[0];
+    if constexpr (kUzClassOrderedK64) {
 #pragma unroll 1
-    for (int color = 0; color < (1 << DIM); color++) {
-        apply_tiles_class<DIM, double, 1, false>(L0.mk, A.mom64, L0.bc, x, A.r64, blockIdx.x, gridDim.x, color);
-        if (!grid_barrier(A.gb, &epoch)) return false;
+        for (int color = 0; color < (1 << DIM); color++) {
+            apply_tiles_class<DIM, double, 1, false>(L0.mk, A.mom64, L0.bc, x, A.r64, blockIdx.x, gridDim.x,
+                                                     color);
+            if (!grid_barrier(A.gb, &epoch)) return false;
+        }
+        return true;
+    } else {
+        apply_tiles<DIM, double, 1, false>(L0.mk, A.mom64, L0.bc, x, A.r64, blockIdx.x, gridDim.x);
+        return grid_barrier(A.gb, &epoch);
     }
-    return true;
 }
 
 // r64 = b − r64 on free rows (0 on Dirichlet rows); returns ‖D⁻¹ r64‖ (every block the
@@ -810,8 +820,8 @@ constexpr int kUzBarrierFail = -1;
 
 // K x = b to ‖D⁻¹(b − Kx)‖ ≤ rtol ‖D⁻¹b‖ (inner_solve's mixed branch): FP32 multigrid
 // flexible-CG sweeps on the FP64 defect, each followed by x += e and the FP64 defect.
-// warm: start from x (else x = 0).  Returns GG_OK / GG_ERR_NOT_CONVERGED /
-// GG_ERR_NONFINITE, or kUzBarrierFail.
+// warm: start from x, whose defect b − Kx the caller has already put in r64 (else
+// x = 0).  Returns GG_OK / GG_ERR_NOT_CONVERGED / GG_ERR_NONFINITE, or kUzBarrierFail.
 template <int DIM>
 __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArgs& A, const double* b, double* x,
                                         double rtol, bool warm, bool& tight, unsigned int& epoch, int& its,
@@ -819,9 +829,10 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
     const FusedLevel& L0 = T.lv[0];
     const int64_t nnode = L0.mk.nnode;
     double* P = A.part + 4 * gridDim.x;
-    // x = 0 and r = b on free rows (the defect of x = 0), or r = 0 for the apply to
-    // accumulate K x0 (warm); the partials of ‖D⁻¹b‖ on free rows either way
-    double acc = 0.0;
+    double* P1 = A.part + 5 * gridDim.x;
+    // x = 0 and r = b on free rows (the defect of x = 0), or the warm start's defect as
+    // given; the partials of ‖D⁻¹b‖ and ‖D⁻¹r‖ on free rows
+    double acc = 0.0, acc_r = 0.0;
     for (int64_t n = gtid(); n < nnode; n += gstride()) {
         const uint8_t bm = L0.bc[n];
 #pragma unroll
@@ -832,43 +843,55 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
             if (!fixed) {
                 const double zv = bv / A.kdiag[i];
                 acc += zv * zv;
+                if (warm) {
+                    const double zr = __ldcg(&A.r64[i]) / A.kdiag[i];
+                    acc_r += zr * zr;
+                }
             }
-            if (!warm) x[i] = 0.0;
-            A.r64[i] = warm ? 0.0 : bv;
+            if (!warm) {
+                x[i] = 0.0;
+                A.r64[i] = bv;
+            }
         }
     }
-    put_partial(acc, P);
+    put_partial2(acc, acc_r, P, P1);
     if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
-    const double rnorm0 = sqrt(all_sum(P));
+    double b2, r2;
+    all_sum2(P, P1, b2, r2);
+    const double rnorm0 = sqrt(b2);
     double ttol = rtol * rnorm0;
     if (ttol < 1e-50) ttol = 1e-50;
     double rn_cur = rnorm0;
-    if (!warm && rnorm0 <= ttol) return GG_OK;
-    // sweep −1 is the warm start's defect; every later turn is an FP32 sweep, x += e and
-    // the FP64 defect (one call site of the FP64 apply and the flexible CG each)
+    if (warm) {
+        const double rn = sqrt(r2);
+        if (!(rn == rn)) return GG_ERR_NONFINITE;
+        if (rn <= ttol) return GG_OK;
+        rn_cur = rn;
+    } else if (rnorm0 <= ttol) {
+        return GG_OK;
+    }
+    // each turn: an FP32 sweep, x += e and the FP64 defect (one call site of the FP64
+    // apply and the flexible CG each)
     int total = 0;
     int rc = GG_ERR_NOT_CONVERGED;
-    for (int sweep = warm ? -1 : 0; sweep < 50; sweep++) {
-        if (sweep >= 0) {
-            const double inner_rtol = tight ? 1e-5 : 1e-4;
-            const double srtol = fmax(inner_rtol, fmin(0.5, ttol / rn_cur));
-            FcgResult res;
-            if (!fcg_body<DIM>(T, nullptr, A.r64, A.e32, A.p32, A.Ap32, srtol, A.sweep_cap, A.part, A.gb, epoch,
-                               res))
-                return kUzBarrierFail;
-            total += res.iterations;
-            sweeps++;
-            if (res.failed >= 2) {
-                rc = GG_ERR_NONFINITE;
-                break;
-            }
-            // x += e, r = 0 for the apply
-            for (int64_t i = gtid(); i < (int64_t)DIM * nnode; i += gstride()) {
-                x[i] = __ldcg(&x[i]) + (double)__ldcg(&A.e32[i]);
-                A.r64[i] = 0.0;
-            }
-            if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
+    for (int sweep = 0; sweep < 50; sweep++) {
+        const double inner_rtol = tight ? 1e-5 : 1e-4;
+        const double srtol = fmax(inner_rtol, fmin(0.5, ttol / rn_cur));
+        FcgResult res;
+        if (!fcg_body<DIM>(T, nullptr, A.r64, A.e32, A.p32, A.Ap32, srtol, A.sweep_cap, A.part, A.gb, epoch, res))
+            return kUzBarrierFail;
+        total += res.iterations;
+        sweeps++;
+        if (res.failed >= 2) {
+            rc = GG_ERR_NONFINITE;
+            break;
         }
+        // x += e, r = 0 for the apply
+        for (int64_t i = gtid(); i < (int64_t)DIM * nnode; i += gstride()) {
+            x[i] = __ldcg(&x[i]) + (double)__ldcg(&A.e32[i]);
+            A.r64[i] = 0.0;
+        }
+        if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
         if (!uz_apply_K64<DIM>(T, A, x, epoch)) return kUzBarrierFail;
         bool ok = true;
         const double rn = uz_defect<DIM>(T, A, b, epoch, &ok);
@@ -883,7 +906,7 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
             break;
         }
         rn_cur = rn;
-        if (sweep >= 0 && total >= A.inner_maxit) break;
+        if (total >= A.inner_maxit) break;
     }
     its += total;
     return rc;
@@ -1056,7 +1079,10 @@ __device__ __forceinline__ bool uzawa_body(const FusedTable& T, const UzawaFused
             A.s[e] = it == 0 ? z : z + beta * __ldcg(&A.s[e]);
         }
         if (!grid_barrier(A.gb, &epoch)) return false;
-        // G s, and the recycled start β u*_prev of K u* = G s
+        // G s, and the recycled start β u*_prev of K u* = G s with its defect: the previous
+        // inner solve ended with r = G s_prev − K u*_prev (its last FP64 defect, still in
+        // r64, ftmp still G s_prev), so G s − K(β u*_prev) = G s − β (G s_prev − r) without
+        // an apply (free rows; 0 on Dirichlet rows)
         const bool warm = A.recycle && it > 0;
         for (int64_t n = gtid(); n < nnode; n += gstride()) {
             double g[DIM];
@@ -1065,8 +1091,13 @@ __device__ __forceinline__ bool uzawa_body(const FusedTable& T, const UzawaFused
 #pragma unroll
             for (int c = 0; c < DIM; c++) {
                 const int64_t i = (int64_t)c * nnode + n;
-                A.ftmp[i] = ((bm >> c) & 1) ? 0.0 : g[c];
-                if (warm) A.vstar[i] = beta * __ldcg(&A.vstar[i]);
+                const bool fixed = (bm >> c) & 1;
+                const double gs = fixed ? 0.0 : g[c];
+                if (warm) {
+                    A.vstar[i] = beta * __ldcg(&A.vstar[i]);
+                    A.r64[i] = fixed ? 0.0 : gs - beta * (__ldcg(&A.ftmp[i]) - __ldcg(&A.r64[i]));
+                }
+                A.ftmp[i] = gs;
             }
         }
         if (!grid_barrier(A.gb, &epoch)) return false;
@@ -1103,15 +1134,17 @@ double program_bytes(const FusedTable& T, const std::vector<FusedPhase>& prog, i
         const int l = P.level;
         const double n = ndof(l), f = 4.0;
         switch (P.type) {
-            case PH_APPLY:
-            case PH_APPLY_P:  // x in, y out, moments, BC bytes
+            case PH_APPLY:  // x in, y out, moments, BC bytes
                 b += 2.0 * n * f + (double)T.lv[l].mk.nel * nm * f + (double)T.lv[l].mk.nnode;
+                break;
+            case PH_APPLY_P:  // + the previous direction read with z
+                b += 3.0 * n * f + (double)T.lv[l].mk.nel * nm * f + (double)T.lv[l].mk.nnode;
                 break;
             case PH_STEP:  // r, t, d, D⁻¹, x in; r, d, x, t out
                 b += 9.0 * n * f;
                 break;
-            case PH_STEP_DOTS:  // + the FCG residual and Ap
-                b += 11.0 * n * f;
+            case PH_STEP_DOTS:  // + the FCG residual and Ap in, Ap zeroed
+                b += 12.0 * n * f;
                 break;
             case PH_RESTRICT:  // fine r, t in; coarse b (and the Chebyshev start) out
                 b += 2.0 * n * f + ndof(l + 1) * f * (P.flag ? 6.0 : 1.0) + (double)T.lv[l + 1].mk.nnode;
@@ -1125,11 +1158,8 @@ double program_bytes(const FusedTable& T, const std::vector<FusedPhase>& prog, i
             case PH_RESTART:  // b, t, D⁻¹, x in; r, d, x, t out
                 b += 8.0 * n * f;
                 break;
-            case PH_DIR:  // z, p in; p, Ap out
-                b += 4.0 * n * f;
-                break;
-            case PH_UPDATE:  // x, p, r, Ap, D⁻¹ in; x, r, level-0 r, d, z, t out
-                b += 11.0 * n * f;
+            case PH_UPDATE:  // x, p, r, Ap, D⁻¹, z in; x, p, r, level-0 r, d, z, t out
+                b += 13.0 * n * f;
                 break;
             default:
                 break;
@@ -1311,7 +1341,6 @@ static int fused_table(Handle& H, const float* b, float* x) {
                 ph(l == 0 && k == dl - 1 ? PH_STEP_DOTS : PH_STEP, l, k);
             }
         }
-        ph(PH_DIR, 0);
         ph(PH_APPLY_P, 0);
         ph(PH_UPDATE, 0);
         if ((int)prog.size() > kMaxPhases) return 1;
