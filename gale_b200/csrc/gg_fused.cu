@@ -95,7 +95,9 @@ struct FusedTable {
     int nphase;    // phases of one iteration
     int coarse_n;
     int vec4;      // every vector of the table and the launch is 16-byte aligned
-    const float* coarse_inv;
+    const float* coarse_inv;  // [coarse_n][coarse_ld], 16-byte aligned rows
+    int coarse_ld;
+    int pad2;
     FusedLevel lv[kFusedMaxLevels];
     FusedPhase ph[kMaxPhases];
 };
@@ -494,12 +496,27 @@ __device__ __forceinline__ void phase_prolong(const FusedLevel& L, const FusedLe
     }
 }
 
-// x = A⁻¹ b on the coarsest level: one warp per row of the dense FP32 inverse
-__device__ __forceinline__ void phase_dense(int n, const float* A, const float* b, float* x) {
+// x = A⁻¹ b on the coarsest level: one warp per row of the dense FP32 inverse, the row
+// (padded to ld, a multiple of 4) and b read as float4 with four independent partial sums;
+// b was written by the restriction before the phase's barrier and is reused by every row,
+// so it is read through L1 (cached weak loads, ordered after that barrier's acquire)
+__device__ __forceinline__ void phase_dense(int n, int ld, const float* A, const float* b, float* x) {
     const int lane = threadIdx.x & 31;
+    const int n4 = n >> 2;
+    const float4* b4 = reinterpret_cast<const float4*>(b);
     for (int64_t row = gtid() >> 5; row < n; row += gstride() >> 5) {
-        float s = 0.f;
-        for (int k = lane; k < n; k += 32) s += A[row * n + k] * __ldcg(&b[k]);
+        const float4* a4 = reinterpret_cast<const float4*>(A + row * ld);
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+        for (int k = lane; k < n4; k += 32) {
+            const float4 av = __ldg(&a4[k]);
+            const float4 bv = __ldca(&b4[k]);
+            s0 += av.x * bv.x;
+            s1 += av.y * bv.y;
+            s2 += av.z * bv.z;
+            s3 += av.w * bv.w;
+        }
+        for (int k = 4 * n4 + lane; k < n; k += 32) s0 += __ldg(&A[row * ld + k]) * __ldca(&b[k]);
+        float s = (s0 + s1) + (s2 + s3);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) x[row] = s;
@@ -631,7 +648,7 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, co
                         phase_restrict<DIM>(L, T.lv[P.level + 1], P.flag != 0);
                     break;
                 case PH_DENSE:
-                    phase_dense(T.coarse_n, T.coarse_inv, L.b, L.x);
+                    phase_dense(T.coarse_n, T.coarse_ld, T.coarse_inv, L.b, L.x);
                     break;
                 case PH_PROLONG:
                     phase_prolong<DIM>(L, T.lv[P.level + 1]);
@@ -1150,7 +1167,7 @@ double program_bytes(const FusedTable& T, const std::vector<FusedPhase>& prog, i
                 b += 2.0 * n * f + ndof(l + 1) * f * (P.flag ? 6.0 : 1.0) + (double)T.lv[l + 1].mk.nnode;
                 break;
             case PH_DENSE:
-                b += (double)T.coarse_n * T.coarse_n * f + 2.0 * T.coarse_n * f;
+                b += (double)T.coarse_n * T.coarse_ld * f + 2.0 * T.coarse_n * f;
                 break;
             case PH_PROLONG:  // coarse x in; fine x in and out, t out
                 b += ndof(l + 1) * f + 3.0 * n * f + (double)T.lv[l].mk.nnode;
@@ -1295,6 +1312,7 @@ static int fused_table(Handle& H, const float* b, float* x) {
         T.nlevels = (int)nl;
         T.coarse_n = (int)H.coarse_n;
         T.coarse_inv = H.coarse_inv.as<float>();
+        T.coarse_ld = (int)H.coarse_ld;
         for (size_t l = 0; l < nl; l++) {
             const MGLevel& L = *H.mg[l];
             FusedLevel& F = T.lv[l];
@@ -1350,6 +1368,8 @@ static int fused_table(Handle& H, const float* b, float* x) {
             const FusedLevel& F = T.lv[l];
             al = al && a16(F.invd) && a16(F.b) && a16(F.x) && a16(F.r) && a16(F.d) && a16(F.t);
         }
+        // the dense phase reads the inverse's rows and the coarsest right-hand side as float4
+        if (!a16(T.coarse_inv) || !a16(T.lv[nl - 1].b) || (T.coarse_ld & 3)) return 1;
         T.vec4 = al ? 1 : 0;
         T.nphase = (int)prog.size();
         H.fused_bytes_it = program_bytes(T, prog, H.nm);

@@ -110,9 +110,10 @@ struct Handle {
     bool mg_ready = false;
     int64_t build_gen = 0;  // incremented by every operator build (graphs bake in its scalars)
     int64_t mg_gen = -1;    // build generation the hierarchy was set up for
-    DBuf coarse_inv;        // dense inverse of the coarsest operator (FP32, [n][n])
+    DBuf coarse_inv;        // dense inverse of the coarsest operator (FP32, [n][ld])
     DBuf mg_part, mg_dense; // power-iteration partials; FP64 columns of the coarsest operator
     int64_t coarse_n = 0;   // 0: no dense coarse solve (Chebyshev on the coarsest level)
+    int64_t coarse_ld = 0;  // row stride of coarse_inv (coarse_n rounded up to 4)
     int mg_degree = 2;      // Chebyshev degree of the smoother
     int build_shape[2] = {-1, -1};  // autotuned CTA shape of the FP64 / FP32 moment build
     // persistent multigrid FCG (gg_fused.cu): level table for the current hierarchy

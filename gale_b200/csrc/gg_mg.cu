@@ -10,8 +10,8 @@
 //     (ξ_coarse = (ξ_child ± 1)/2), so every level is matrix-free with the same kernel;
 //   * smoothing is Chebyshev–Jacobi (eigen-bound from a power iteration), which is a
 //     fixed polynomial of D⁻¹A — no inner products inside the V-cycle;
-//   * the coarsest level (≤ 400 dofs) is solved by a dense FP32 inverse (one mat-vec),
-//     computed on the device by Gauss–Jordan;
+//   * the coarsest level (≤ 3000 dofs) is solved by a dense FP32 inverse (one mat-vec),
+//     computed on the device by blocked Gauss–Jordan;
 //   * the whole V-cycle is a fixed kernel sequence and is captured into the inner
 //     Krylov iteration's CUDA graph; every kernel exits early once the solve is done.
 // The V-cycle preconditions a flexible CG (Notay's truncated FCG) so that the learned
@@ -26,7 +26,6 @@
 
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
-#include "gg_grid.cuh"
 #include "gg_ops.cuh"
 
 namespace gg {
@@ -36,10 +35,12 @@ MeshK make_mesh(const gg_mesh_desc& d);
 namespace {
 
 constexpr int kMinCoarse = 4;      // coarsen while every axis is even and ≥ 4 elements
-// … and the level has more dofs than this: the dense inverse of the coarsest level is
-// rebuilt at every operator build (Picard iterations included) by device Gauss–Jordan,
-// n launches of O(n²) work, so its size stays a few hundred dofs
-constexpr int64_t kDenseStop = 400;
+// … and the level has more dofs than this.  The dense inverse of the coarsest level is
+// rebuilt at every operator build (Picard iterations included) by blocked Gauss–Jordan
+// (n³ FP64 multiply-adds); one dense mat-vec then replaces the V-cycle's levels below it,
+// each of whose phases is bound by latency, not work (64³: 8³ = 2,187 dofs is the
+// coarsest level, and the 8³ and 4³ cycles' ten phases per iteration become one)
+constexpr int64_t kDenseStop = 3000;
 
 __device__ __forceinline__ double tcoef(int a, int ap, double o) {
     // ξ_c = (ξ_f + o)/2  ⇒  ξ_c^a = Σ_{a'≤a} T[a][a'] ξ_f^{a'}
@@ -290,14 +291,15 @@ __global__ void k_resid_finish(int64_t n, float* __restrict__ r, float* __restri
     }
 }
 
-// x = A⁻¹ b on the coarsest level: one warp per row of the dense FP32 inverse
-__global__ void k_dense_mv(int n, const float* __restrict__ A, const float* __restrict__ b, float* __restrict__ x,
-                           const int32_t* __restrict__ done) {
+// x = A⁻¹ b on the coarsest level: one warp per row of the dense FP32 inverse (rows
+// padded to ld)
+__global__ void k_dense_mv(int n, int ld, const float* __restrict__ A, const float* __restrict__ b,
+                           float* __restrict__ x, const int32_t* __restrict__ done) {
     if (done && *done) return;
     const int lane = threadIdx.x & 31;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += (gridDim.x * blockDim.x) >> 5) {
         float s = 0.f;
-        for (int k = lane; k < n; k += 32) s += A[(int64_t)row * n + k] * b[k];
+        for (int k = lane; k < n; k += 32) s += A[(int64_t)row * ld + k] * b[k];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) x[row] = s;
@@ -397,7 +399,8 @@ void vcycle(Handle& H, size_t l, const float* b, float* x, const int32_t* done) 
     const int dim = H.dim;
     if (l + 1 == H.mg.size()) {
         if (H.coarse_n) {
-            k_dense_mv<<<g((int64_t)H.coarse_n * 32), 256, 0, st>>>((int)H.coarse_n, H.coarse_inv.as<float>(), b, x, done);
+            k_dense_mv<<<g((int64_t)H.coarse_n * 32), 256, 0, st>>>((int)H.coarse_n, (int)H.coarse_ld,
+                                                                   H.coarse_inv.as<float>(), b, x, done);
             H.kernel_launches++;
             return;
         }
@@ -489,68 +492,171 @@ static double power_lambda(Handle& H, MGLevel& L) {
     return lam;
 }
 
-// Dense inverse of the coarsest level: columns K e_j from the matrix-free apply (FP64),
-// then Gauss–Jordan on the device.
-// [A | I] with the BC rows and columns of A replaced by the identity (A symmetric:
-// column j of K was written to A + j·n)
-__global__ void k_gj_init(int64_t n, int64_t nnode, const uint8_t* __restrict__ bc, const double* __restrict__ A,
-                          double* __restrict__ M) {
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * 2 * n;
-         q += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = q / (2 * n), k = q - i * 2 * n;
-        double v;
-        if (k < n) {
-            const int ci = (int)(i / nnode), ck = (int)(k / nnode);
-            const bool fi = (bc[i - ci * nnode] >> ci) & 1, fk = (bc[k - ck * nnode] >> ck) & 1;
-            v = (fi || fk) ? (i == k ? 1.0 : 0.0) : A[k * n + i];
-        } else {
-            v = (k - n == i) ? 1.0 : 0.0;
-        }
-        M[q] = v;
-    }
-}
+// ---- blocked Gauss–Jordan inversion, in place, FP64 ------------------------------------
+// For pivot blocks K = [k0, k0 + b) in turn (b ≤ kGjB), with D = W[K,K]:
+//   W[i,j] −= W[i,K] D⁻¹ W[K,j]   (i, j ∉ K)      W[K,j] = D⁻¹ W[K,j]   (j ∉ K)
+//   W[i,K]  = −W[i,K] D⁻¹         (i ∉ K)         W[K,K] = D⁻¹
+// after the last block W holds the inverse.  No pivoting: every leading Schur complement
+// of a symmetric positive definite matrix is symmetric positive definite.  The work is a
+// rank-b update of the whole matrix per block (n³ multiply-adds in all, on the SMs' FP64
+// units from shared-memory tiles); the only sequential part is the b steps inside each
+// diagonal block, n steps in all.
+constexpr int kGjB = 64;      // pivot block
+constexpr int kGjTile = 128;  // output tile of the update (256 threads × 8 × 8)
 
-// One Gauss–Jordan step on pivot c, reading `in` and writing `out` (no pivoting: the
-// matrix is symmetric positive definite): row c / a_cc, every other row minus its
-// multiple of the pivot row.
-__global__ void k_gj_step(int64_t n, int64_t c, const double* __restrict__ in, double* __restrict__ out) {
-    const int64_t w = 2 * n;
-    const double inv_p = 1.0 / in[c * w + c];
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * w; q += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = q / w, k = q - i * w;
-        const double pk = in[c * w + k] * inv_p;
-        out[q] = i == c ? pk : in[q] - in[i * w + c] * pk;
-    }
-}
-
-// All n Gauss–Jordan steps in one cooperative launch: step c reads `in` and writes `out` as
-// k_gj_step does, then the grid meets at a barrier and the buffers swap.  `in` was written
-// by other blocks in this launch, so it is read through L2 (ld.global.cg).  A barrier that
-// gives up (error word in gb) ends every block; the host reports it.
-__global__ void k_gj_all(int64_t n, double* __restrict__ m0, double* __restrict__ m1, GridBarrier* gb) {
-    unsigned int epoch = 0;
-    const int64_t w = 2 * n;
-    double* in = m0;
-    double* out = m1;
-    for (int64_t c = 0; c < n; c++) {
-        const double inv_p = 1.0 / __ldcg(&in[c * w + c]);
-        for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * w;
-             q += (int64_t)gridDim.x * blockDim.x) {
-            const int64_t i = q / w, k = q - i * w;
-            const double pk = __ldcg(&in[c * w + k]) * inv_p;
-            out[q] = i == c ? pk : __ldcg(&in[q]) - __ldcg(&in[i * w + c]) * pk;
-        }
-        if (!grid_barrier(gb, &epoch)) return;
-        double* t = in;
-        in = out;
-        out = t;
-    }
-}
-
-__global__ void k_gj_extract(int64_t n, const double* __restrict__ M, float* __restrict__ inv) {
+// W = A as rows (A holds the columns K e_j; K is symmetric up to the order of its FP64
+// sums, and the transpose keeps W = K exactly), BC rows and columns replaced by the identity
+__global__ void k_bgj_init(int64_t n, int64_t nnode, const uint8_t* __restrict__ bc, const double* __restrict__ A,
+                           double* __restrict__ W) {
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * n; q += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = q / n, k = q - i * n;
-        inv[q] = (float)M[i * 2 * n + n + k];
+        const int64_t i = q / n, j = q - i * n;
+        const int ci = (int)(i / nnode), cj = (int)(j / nnode);
+        const bool fi = (bc[i - ci * nnode] >> ci) & 1, fj = (bc[j - cj * nnode] >> cj) & 1;
+        W[q] = (fi || fj) ? (i == j ? 1.0 : 0.0) : A[j * n + i];
+    }
+}
+
+// D⁻¹ of the pivot block by element-wise Gauss–Jordan steps in shared memory: one CTA of
+// 1024 threads, thread t owning entries t + 1024·r (r < 4) of the block padded to 64 × 64
+// with the identity (the padded inverse holds D⁻¹ in its top left b × b).  Each step
+// reads one copy of the block and writes the other (one barrier per step); the row
+// stride of 65 doubles keeps the pivot-column reads free of bank conflicts.
+constexpr size_t kGjPivotSmem = sizeof(double) * 2 * kGjB * (kGjB + 1);
+__global__ void __launch_bounds__(1024) k_bgj_pivot(int64_t n, int64_t k0, int b, const double* __restrict__ W,
+                                                    double* __restrict__ Dinv) {
+    extern __shared__ double s_piv[];
+    constexpr int S = kGjB + 1;
+    double* D0 = s_piv;
+    double* D1 = s_piv + kGjB * S;
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int q = t + 1024 * r, i = q >> 6, j = q & 63;
+        D0[i * S + j] = (i < b && j < b) ? W[(k0 + i) * n + k0 + j] : (i == j ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    for (int p = 0; p < kGjB; p++) {
+        const double* D = (p & 1) ? D1 : D0;
+        double* E = (p & 1) ? D0 : D1;
+        const double piv = 1.0 / D[p * S + p];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int q = t + 1024 * r, i = q >> 6, j = q & 63;
+            double v;
+            if (i == p) v = j == p ? piv : D[p * S + j] * piv;
+            else v = j == p ? -D[i * S + p] * piv : D[i * S + j] - D[i * S + p] * (D[p * S + j] * piv);
+            E[i * S + j] = v;
+        }
+        __syncthreads();
+    }
+    const double* D = (kGjB & 1) ? D1 : D0;  // after 64 steps the result is back in D0
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int q = t + 1024 * r, i = q >> 6, j = q & 63;
+        if (i < b && j < b) Dinv[i * b + j] = D[i * S + j];
+    }
+}
+
+// The pivot block's row panel R[m][j] = (D⁻¹ W[K,:])[m][j] (columns j ∈ K: D⁻¹ itself) and
+// a copy of its column panel, stored transposed CT[m][i] = W[i][k0+m], both from W before
+// the update
+__global__ void k_bgj_panels(int64_t n, int64_t k0, int b, const double* __restrict__ W,
+                             const double* __restrict__ Dinv, double* __restrict__ R, double* __restrict__ C) {
+    const int64_t nb = (int64_t)b * n;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < 2 * nb; q += (int64_t)gridDim.x * blockDim.x) {
+        if (q < nb) {
+            const int m = (int)(q / n);
+            const int64_t j = q - (int64_t)m * n;
+            double s;
+            if (j >= k0 && j < k0 + b) {
+                s = Dinv[m * b + (j - k0)];
+            } else {
+                s = 0.0;
+                for (int l = 0; l < b; l++) s += Dinv[m * b + l] * W[(k0 + l) * n + j];
+            }
+            R[m * n + j] = s;
+        } else {
+            const int64_t r = q - nb, i = r / b;
+            const int m = (int)(r - i * b);
+            C[(int64_t)m * n + i] = W[i * n + k0 + m];
+        }
+    }
+}
+
+// The rank-b update of one 128 × 128 output tile (blockIdx.x, blockIdx.y = column, row
+// tile): rows in K take the row panel, every other row W[i,j] (or 0 for j ∈ K) minus
+// C[i,:]·R[:,j].  C (stored transposed) and R tiles are staged in shared memory by
+// coalesced loads; each thread forms an 8 × 8 block of outputs (rows 4·ty + {0..3} and
+// 64 + 4·ty + {0..3}, columns likewise with tx), so a warp's shared-memory reads are
+// broadcasts or consecutive.
+constexpr size_t kGjUpdateSmem = sizeof(double) * 2 * kGjB * kGjTile;
+__global__ void __launch_bounds__(256, 1) k_bgj_update(int64_t n, int64_t k0, int b, double* __restrict__ W,
+                                                       const double* __restrict__ R, const double* __restrict__ C) {
+    extern __shared__ double s_bgj[];
+    double* Cs = s_bgj;                   // [kGjB][kGjTile]
+    double* Rs = s_bgj + kGjB * kGjTile;  // [kGjB][kGjTile]
+    const int64_t i0 = (int64_t)blockIdx.y * kGjTile, j0 = (int64_t)blockIdx.x * kGjTile;
+    for (int q = threadIdx.x; q < kGjB * kGjTile; q += blockDim.x) {
+        const int m = q / kGjTile, t = q % kGjTile;
+        const bool ok = m < b;
+        Cs[q] = ok && i0 + t < n ? C[(int64_t)m * n + i0 + t] : 0.0;
+        Rs[q] = ok && j0 + t < n ? R[(int64_t)m * n + j0 + t] : 0.0;
+    }
+    __syncthreads();
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    double acc[8][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+        for (int c = 0; c < 8; c++) acc[r][c] = 0.0;
+    for (int m = 0; m < b; m++) {
+        const double* cm = Cs + m * kGjTile;
+        const double* rm = Rs + m * kGjTile;
+        double cv[8], rv[8];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const double2 c01 = *reinterpret_cast<const double2*>(cm + 64 * h + 4 * ty);
+            const double2 c23 = *reinterpret_cast<const double2*>(cm + 64 * h + 4 * ty + 2);
+            const double2 r01 = *reinterpret_cast<const double2*>(rm + 64 * h + 4 * tx);
+            const double2 r23 = *reinterpret_cast<const double2*>(rm + 64 * h + 4 * tx + 2);
+            cv[4 * h] = c01.x;
+            cv[4 * h + 1] = c01.y;
+            cv[4 * h + 2] = c23.x;
+            cv[4 * h + 3] = c23.y;
+            rv[4 * h] = r01.x;
+            rv[4 * h + 1] = r01.y;
+            rv[4 * h + 2] = r23.x;
+            rv[4 * h + 3] = r23.y;
+        }
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+#pragma unroll
+            for (int c = 0; c < 8; c++) acc[r][c] += cv[r] * rv[c];
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const int64_t i = i0 + 64 * (r >> 2) + 4 * ty + (r & 3);
+        if (i >= n) continue;
+        const bool rowK = i >= k0 && i < k0 + b;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int64_t j = j0 + 64 * (c >> 2) + 4 * tx + (c & 3);
+            if (j >= n) continue;
+            if (rowK) {
+                W[i * n + j] = R[(i - k0) * n + j];
+            } else {
+                const double base = (j >= k0 && j < k0 + b) ? 0.0 : W[i * n + j];
+                W[i * n + j] = base - acc[r][c];
+            }
+        }
+    }
+}
+
+// the FP32 inverse with rows padded to ld (a multiple of 4) for float4 mat-vecs
+__global__ void k_bgj_extract(int64_t n, int64_t ld, const double* __restrict__ W, float* __restrict__ inv) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n * ld; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q / ld, j = q - i * ld;
+        inv[q] = j < n ? (float)W[i * n + j] : 0.f;
     }
 }
 
@@ -594,63 +700,49 @@ __global__ void k_coarse_columns(MeshK mk, const double* __restrict__ mom, const
     }
 }
 
+// Dense FP32 inverse of the coarsest operator: its columns by unit-vector applies (FP64),
+// then the blocked Gauss–Jordan inversion above (FP64), rounded to FP32 with rows padded
+// to a multiple of 4.  3 launches per pivot block of 64: C2's 8³ level (2,187 dofs) takes
+// 35 blocks.
 static void coarse_inverse(Handle& H, MGLevel& L) {
     const int64_t n = L.ndof;
+    const int64_t ld = (n + 3) & ~(int64_t)3;
     cudaStream_t st = H.stream;
-    H.mg_dense.ensure(sizeof(double) * (n * n + n + 4 * n * n));
+    H.mg_dense.ensure(sizeof(double) * (2 * n * n + 2 * n * kGjB + kGjB * kGjB));
     double* A = H.mg_dense.as<double>();
-    double* e = A + n * n;
-    double* M0 = e + n;
-    double* M1 = M0 + 2 * n * n;
-    (void)e;
+    double* W = A + n * n;
+    double* R = W + n * n;
+    double* Cp = R + n * kGjB;
+    double* Dinv = Cp + n * kGjB;
     GG_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * n * n, st));
     const int64_t threads = L.nel * (int64_t)(H.dim == 3 ? 24 : 8);
     if (H.dim == 3) k_coarse_columns<3><<<grid_for(threads, 128), 128, 0, st>>>(L.mk, L.mom64, L.bcmask, A);
     else k_coarse_columns<2><<<grid_for(threads, 128), 128, 0, st>>>(L.mk, L.mom64, L.bcmask, A);
-    H.kernel_launches++;
-    const int gb = grid_for(2 * n * n, 256);
-    k_gj_init<<<gb, 256, 0, st>>>(n, L.nnode, L.bcmask, A, M0);
-    // one cooperative launch with a grid barrier between steps where the device allows it
-    // (n barriers of ~2 µs instead of n launches); else one launch per step
-    static std::atomic<int> coop_blocks[64];  // co-resident blocks of k_gj_all per device (0: not probed)
+    k_bgj_init<<<grid_for(n * n, 256), 256, 0, st>>>(n, L.nnode, L.bcmask, A, W);
+    static std::atomic<bool> smem_set[64];
     int dev = 0;
     GG_CUDA(cudaGetDevice(&dev));
-    int coop = 0;
-    if (dev >= 0 && dev < 64) {
-        if (coop_blocks[dev].load() == 0) {
-            int attr = 0, per_sm = 0;
-            GG_CUDA(cudaDeviceGetAttribute(&attr, cudaDevAttrCooperativeLaunch, dev));
-            if (attr) GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_all, 256, 0));
-            coop_blocks[dev].store(attr && per_sm > 0 ? per_sm * num_sms() : -1);
-        }
-        coop = coop_blocks[dev].load();
+    if (dev >= 0 && dev < 64 && !smem_set[dev].load()) {
+        GG_CUDA(cudaFuncSetAttribute(k_bgj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjUpdateSmem));
+        GG_CUDA(cudaFuncSetAttribute(k_bgj_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjPivotSmem));
+        smem_set[dev].store(true);
     }
-    if (coop > 0) {
-        const int grid = std::min(coop, gb);
-        H.fused_bar.ensure(sizeof(GridBarrier));
-        GridBarrier* bar = H.fused_bar.as<GridBarrier>();
-        GG_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), st));
-        int64_t nn = n;
-        void* args[] = {(void*)&nn, (void*)&M0, (void*)&M1, (void*)&bar};
-        GG_CUDA(cudaLaunchCooperativeKernel((const void*)k_gj_all, dim3(grid), dim3(256), args, 0, st));
-        GridBarrier hb{};
-        GG_CUDA(cudaMemcpyAsync(&hb, bar, sizeof(GridBarrier), cudaMemcpyDeviceToHost, st));
-        GG_CUDA(cudaStreamSynchronize(st));
-        if (hb.err) throw CudaError(cudaErrorLaunchTimeout, "k_gj_all grid barrier gave up", __FILE__, __LINE__);
-        if (n & 1) std::swap(M0, M1);  // the last step wrote the other buffer
-        H.kernel_launches += 1 - n;    // one launch instead of n (counted below)
-    } else {
-        for (int64_t c = 0; c < n; c++) {
-            k_gj_step<<<gb, 256, 0, st>>>(n, c, M0, M1);
-            std::swap(M0, M1);
-        }
+    const dim3 tiles((unsigned)((n + kGjTile - 1) / kGjTile), (unsigned)((n + kGjTile - 1) / kGjTile));
+    int64_t launches = 0;
+    for (int64_t k0 = 0; k0 < n; k0 += kGjB) {
+        const int b = (int)std::min<int64_t>(kGjB, n - k0);
+        k_bgj_pivot<<<1, 1024, kGjPivotSmem, st>>>(n, k0, b, W, Dinv);
+        k_bgj_panels<<<grid_for(2 * (int64_t)b * n, 256), 256, 0, st>>>(n, k0, b, W, Dinv, R, Cp);
+        k_bgj_update<<<tiles, 256, kGjUpdateSmem, st>>>(n, k0, b, W, R, Cp);
+        launches += 3;
     }
-    H.coarse_inv.ensure(sizeof(float) * n * n);
-    k_gj_extract<<<grid_for(n * n, 256), 256, 0, st>>>(n, M0, H.coarse_inv.as<float>());
+    H.coarse_inv.ensure(sizeof(float) * n * ld);
+    k_bgj_extract<<<grid_for(n * ld, 256), 256, 0, st>>>(n, ld, W, H.coarse_inv.as<float>());
     GG_CUDA(cudaGetLastError());
-    H.kernel_launches += n + 2;
+    H.kernel_launches += launches + 3;
     GG_CUDA(cudaStreamSynchronize(st));
     H.coarse_n = n;
+    H.coarse_ld = ld;
 }
 
 // Build (or refresh for a new operator) the hierarchy.  Needs the mixed build (FP32 moments).
@@ -721,7 +813,7 @@ int mg_setup(Handle& H) {
     H.kernel_launches += 1 + 4 * (int64_t)(H.mg.size() - 1);
     MGLevel& Lc = *H.mg.back();
     H.coarse_n = 0;
-    if (H.mg.size() > 1 && Lc.ndof <= 3000) coarse_inverse(H, Lc);
+    if (H.mg.size() > 1 && Lc.ndof <= kDenseStop) coarse_inverse(H, Lc);
     GG_CUDA(cudaStreamSynchronize(st));
     H.mg_gen = H.build_gen;
     return GG_OK;
