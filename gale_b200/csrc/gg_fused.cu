@@ -497,7 +497,7 @@ __device__ __forceinline__ void phase_prolong(const FusedLevel& L, const FusedLe
 }
 
 // x = A⁻¹ b on the coarsest level: one warp per row of the dense FP32 inverse, the row
-// (padded to ld, a multiple of 4) and b read as float4 with four independent partial sums;
+// (padded to ld, a multiple of 4) and b read as float4 into four partial sums;
 // b was written by the restriction before the phase's barrier and is reused by every row,
 // so it is read through L1 (cached weak loads, ordered after that barrier's acquire)
 __device__ __forceinline__ void phase_dense(int n, int ld, const float* A, const float* b, float* x) {
@@ -595,13 +595,32 @@ struct FcgResult {
     int failed;  // 0 converged, 1 iteration cap, 2 non-finite residual, 3 pᵀAp ≤ 0
 };
 
+// The start of a flexible-CG solve for dof i of level 0 with right-hand side value rv
+// (0 on Dirichlet rows): x = p = Ap = 0, r = rv and the level-0 Chebyshev start — what
+// phase_update_start does when update = false.  For a caller that folds the start into a
+// phase of its own; the caller also writes Σ rv² per block into part[0, gridDim.x).
+__device__ __forceinline__ void fcg_start_dof(const FusedLevel& L0, int64_t i, float rv, float* x, float* p,
+                                              float* Ap) {
+    x[i] = 0.f;
+    p[i] = 0.f;
+    Ap[i] = 0.f;
+    L0.b[i] = rv;
+    const float dv = L0.inv_theta * L0.invd[i] * rv;
+    L0.r[i] = rv;
+    L0.d[i] = dv;
+    L0.x[i] = dv;
+    L0.t[i] = 0.f;
+}
+
 // The whole solve of K32 x = b to ‖r‖ ≤ rtol‖b‖ from x = 0, within a launch whose barrier
 // count is `epoch`; b is FP32, or FP64 (b64 non-null: rounded to FP32 as it is read).
+// prestarted: the caller has made the start (fcg_start_dof for every dof, the Σ r²
+// partials in part[0, gridDim.x)) in a phase that ended with a grid barrier.
 // Uses part[0, 4·gridDim.x).  Returns false if a barrier gave up.
 template <int DIM>
 __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, const double* b64, float* x, float* p,
                                          float* Ap, double rtol, int maxit, double* part, GridBarrier* gb,
-                                         unsigned int& epoch, FcgResult& res) {
+                                         unsigned int& epoch, FcgResult& res, bool prestarted = false) {
     const FusedLevel& L0 = T.lv[0];
     const int64_t n = (int64_t)DIM * L0.mk.nnode;
     const int G = gridDim.x;
@@ -610,8 +629,10 @@ __device__ __forceinline__ bool fcg_body(const FusedTable& T, const float* b, co
     double* p_zap = part + 2 * G;
     double* p_pap = part + 3 * G;
     const bool vec = T.vec4 != 0;
-    put_partial(phase_update_start<DIM>(L0, false, 0.f, 0.f, b, b64, x, p, Ap, vec), p_rr);
-    if (!grid_barrier(gb, &epoch)) return false;
+    if (!prestarted) {
+        put_partial(phase_update_start<DIM>(L0, false, 0.f, 0.f, b, b64, x, p, Ap, vec), p_rr);
+        if (!grid_barrier(gb, &epoch)) return false;
+    }
     const double rnorm0 = sqrt(all_sum(p_rr));
     const double tt = rtol * rnorm0;
     const double ttol = tt < 1e-30 ? 1e-30 : tt;
@@ -768,6 +789,7 @@ struct UzawaFusedArgs {
     const double* f;
     const double* hv;
     double *u, *vstar, *ftmp, *q, *qtmp, *r, *s, *r64;
+    double* acc64;  // FP64 apply accumulator (zero between sweeps)
     float *e32, *p32, *Ap32;
     double tolerance, inner_rtol, scaleq;
     double floor_u, floor_h;  // the exact-flow test: ‖r0‖ ≤ floor_u ‖u‖ + floor_h ‖h‖
@@ -778,42 +800,34 @@ struct UzawaFusedArgs {
     GridBarrier* gb;
 };
 
-// The FP64 apply of the defect: true sums every node's element terms in parity-class order
-// (one phase per class, the same bits on every run); false scatters all elements in one
-// phase with FP64 atomics (arrival order).  The mixed path's iterates already depend on the
-// FP32 atomics' order, so it takes the one-phase apply: measured on creep 64³ (136 outer
-// iterations, 692 flexible-CG iterations), the solve's FP64 applies cost 30.6 ms in class
-// order and 11.5 ms in one phase.
-constexpr bool kUzClassOrderedK64 = false;
-
-// r64 = K x (r64 zero on entry).  False if a barrier gave up.
+// acc64 += K (x + e): the FP64 iterate plus the sweep's FP32 correction, added at the
+// element gather (x itself is updated in the defect phase that follows), all elements in
+// one phase with FP64 atomics (arrival order).  Summed in element parity-class order
+// instead (one phase per class, as the plain FP64 path does), the FP64 applies of the
+// creep 64³ solve (136 outer, 692 flexible-CG iterations) took 30.6 ms against 11.5 ms;
+// the mixed path's iterates already depend on the FP32 atomics' order.  acc64 is zero on
+// entry.  False if a barrier gave up.
 template <int DIM>
 __device__ __forceinline__ bool uz_apply_K64(const FusedTable& T, const UzawaFusedArgs& A, const double* x,
                                              unsigned int& epoch) {
     const FusedLevel& L0 = T.lv[0];
-    if constexpr (kUzClassOrderedK64) {
-#pragma unroll 1
-        for (int color = 0; color < (1 << DIM); color++) {
-            apply_tiles_class<DIM, double, 1, false>(L0.mk, A.mom64, L0.bc, x, A.r64, blockIdx.x, gridDim.x,
-                                                     color);
-            if (!grid_barrier(A.gb, &epoch)) return false;
-        }
-        return true;
-    } else {
-        apply_tiles<DIM, double, 1, false>(L0.mk, A.mom64, L0.bc, x, A.r64, blockIdx.x, gridDim.x);
-        return grid_barrier(A.gb, &epoch);
-    }
+    apply_tiles<DIM, double, 1, false, ApplyTile<DIM>::Y, ApplyTile<DIM>::Z, true, float>(
+        L0.mk, A.mom64, L0.bc, x, A.acc64, blockIdx.x, gridDim.x, A.e32, 1.0);
+    return grid_barrier(A.gb, &epoch);
 }
 
-// r64 = b − r64 on free rows (0 on Dirichlet rows); returns ‖D⁻¹ r64‖ (every block the
-// same value).  *ok = false if the barrier gave up.
+// The defect phase after a sweep: r64 = b − acc64 on free rows (0 on Dirichlet rows),
+// acc64 = 0 for the next apply, x += e; and, speculatively, the next sweep's flexible-CG
+// start on that defect (fcg_start_dof; it is simply overwritten if the solve has
+// converged).  Returns ‖D⁻¹ r64‖ (every block the same value); the Σ r² partials of the
+// start are in part[0, gridDim.x).  *ok = false if the barrier gave up.
 template <int DIM>
-__device__ __forceinline__ double uz_defect(const FusedTable& T, const UzawaFusedArgs& A, const double* b,
-                                            unsigned int& epoch, bool* ok) {
+__device__ __forceinline__ double uz_defect_start(const FusedTable& T, const UzawaFusedArgs& A, const double* b,
+                                                  double* x, unsigned int& epoch, bool* ok) {
     const FusedLevel& L0 = T.lv[0];
     const int64_t nnode = L0.mk.nnode;
     double* P = A.part + 4 * gridDim.x;
-    double acc = 0.0;
+    double acc = 0.0, acc32 = 0.0;
     for (int64_t n = gtid(); n < nnode; n += gstride()) {
         const uint8_t bm = L0.bc[n];
 #pragma unroll
@@ -821,14 +835,19 @@ __device__ __forceinline__ double uz_defect(const FusedTable& T, const UzawaFuse
             const int64_t i = (int64_t)c * nnode + n;
             double rv = 0.0;
             if (!((bm >> c) & 1)) {
-                rv = __ldcg(&b[i]) - __ldcg(&A.r64[i]);
+                rv = __ldcg(&b[i]) - __ldcg(&A.acc64[i]);
                 const double zv = rv / A.kdiag[i];
                 acc += zv * zv;
             }
             A.r64[i] = rv;
+            A.acc64[i] = 0.0;
+            x[i] = __ldcg(&x[i]) + (double)__ldcg(&A.e32[i]);
+            const float r32 = (float)rv;
+            fcg_start_dof(L0, i, r32, A.e32, A.p32, A.Ap32);
+            acc32 += (double)r32 * (double)r32;
         }
     }
-    put_partial(acc, P);
+    put_partial2(acc, acc32, P, A.part);
     *ok = grid_barrier(A.gb, &epoch);
     return *ok ? sqrt(all_sum(P)) : 0.0;
 }
@@ -836,9 +855,11 @@ __device__ __forceinline__ double uz_defect(const FusedTable& T, const UzawaFuse
 constexpr int kUzBarrierFail = -1;
 
 // K x = b to ‖D⁻¹(b − Kx)‖ ≤ rtol ‖D⁻¹b‖ (inner_solve's mixed branch): FP32 multigrid
-// flexible-CG sweeps on the FP64 defect, each followed by x += e and the FP64 defect.
+// flexible-CG sweeps on the FP64 defect, each followed by the FP64 defect of x + e.
 // warm: start from x, whose defect b − Kx the caller has already put in r64 (else
-// x = 0).  Returns GG_OK / GG_ERR_NOT_CONVERGED / GG_ERR_NONFINITE, or kUzBarrierFail.
+// x = 0).  Each phase that ends with a defect also makes the next sweep's start, so a
+// sweep costs its FCG iterations plus two phases (the FP64 apply and the defect).
+// Returns GG_OK / GG_ERR_NOT_CONVERGED / GG_ERR_NONFINITE, or kUzBarrierFail.
 template <int DIM>
 __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArgs& A, const double* b, double* x,
                                         double rtol, bool warm, bool& tight, unsigned int& epoch, int& its,
@@ -848,8 +869,9 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
     double* P = A.part + 4 * gridDim.x;
     double* P1 = A.part + 5 * gridDim.x;
     // x = 0 and r = b on free rows (the defect of x = 0), or the warm start's defect as
-    // given; the partials of ‖D⁻¹b‖ and ‖D⁻¹r‖ on free rows
-    double acc = 0.0, acc_r = 0.0;
+    // given; acc64 = 0; the first sweep's start on r; the partials of ‖D⁻¹b‖, ‖D⁻¹r‖ and
+    // the start's Σ r²
+    double acc = 0.0, acc_r = 0.0, acc32 = 0.0;
     for (int64_t n = gtid(); n < nnode; n += gstride()) {
         const uint8_t bm = L0.bc[n];
 #pragma unroll
@@ -857,21 +879,26 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
             const int64_t i = (int64_t)c * nnode + n;
             const bool fixed = (bm >> c) & 1;
             const double bv = fixed ? 0.0 : __ldcg(&b[i]);
+            double rv = bv;
+            if (warm) rv = fixed ? 0.0 : __ldcg(&A.r64[i]);
             if (!fixed) {
                 const double zv = bv / A.kdiag[i];
                 acc += zv * zv;
-                if (warm) {
-                    const double zr = __ldcg(&A.r64[i]) / A.kdiag[i];
-                    acc_r += zr * zr;
-                }
+                const double zr = rv / A.kdiag[i];
+                acc_r += zr * zr;
             }
             if (!warm) {
                 x[i] = 0.0;
                 A.r64[i] = bv;
             }
+            A.acc64[i] = 0.0;
+            const float r32 = (float)rv;
+            fcg_start_dof(L0, i, r32, A.e32, A.p32, A.Ap32);
+            acc32 += (double)r32 * (double)r32;
         }
     }
     put_partial2(acc, acc_r, P, P1);
+    put_partial(acc32, A.part);
     if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
     double b2, r2;
     all_sum2(P, P1, b2, r2);
@@ -887,15 +914,14 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
     } else if (rnorm0 <= ttol) {
         return GG_OK;
     }
-    // each turn: an FP32 sweep, x += e and the FP64 defect (one call site of the FP64
-    // apply and the flexible CG each)
     int total = 0;
     int rc = GG_ERR_NOT_CONVERGED;
     for (int sweep = 0; sweep < 50; sweep++) {
         const double inner_rtol = tight ? 1e-5 : 1e-4;
         const double srtol = fmax(inner_rtol, fmin(0.5, ttol / rn_cur));
         FcgResult res;
-        if (!fcg_body<DIM>(T, nullptr, A.r64, A.e32, A.p32, A.Ap32, srtol, A.sweep_cap, A.part, A.gb, epoch, res))
+        if (!fcg_body<DIM>(T, nullptr, A.r64, A.e32, A.p32, A.Ap32, srtol, A.sweep_cap, A.part, A.gb, epoch, res,
+                           true))
             return kUzBarrierFail;
         total += res.iterations;
         sweeps++;
@@ -903,15 +929,9 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
             rc = GG_ERR_NONFINITE;
             break;
         }
-        // x += e, r = 0 for the apply
-        for (int64_t i = gtid(); i < (int64_t)DIM * nnode; i += gstride()) {
-            x[i] = __ldcg(&x[i]) + (double)__ldcg(&A.e32[i]);
-            A.r64[i] = 0.0;
-        }
-        if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
         if (!uz_apply_K64<DIM>(T, A, x, epoch)) return kUzBarrierFail;
         bool ok = true;
-        const double rn = uz_defect<DIM>(T, A, b, epoch, &ok);
+        const double rn = uz_defect_start<DIM>(T, A, b, x, epoch, &ok);
         if (!ok) return kUzBarrierFail;
         if (!(rn == rn)) {
             rc = GG_ERR_NONFINITE;
@@ -1471,6 +1491,7 @@ int run_uzawa_fused(Handle& H, const gg_uzawa_params& prm, gg_uzawa_stats& S) {
     A.r = H.r.as<double>();
     A.s = H.s.as<double>();
     A.r64 = H.cg_r.as<double>();
+    A.acc64 = H.cg_z.as<double>();
     A.e32 = H.e32.as<float>();
     A.p32 = H.p32.as<float>();
     A.Ap32 = H.Ap32.as<float>();

@@ -154,13 +154,13 @@ __device__ __forceinline__ double element_compute_scatter(const MeshK& mk, R (&m
 }
 
 // kAxpy: the nodal values are x + beta·x2, formed at the gather (a flexible-CG direction
-// p = z + βp applied without storing it first).
-template <int DIM, typename R, int kLoad = 0, bool kEnergy = true, bool kAxpy = false>
+// p = z + βp applied without storing it first; an FP64 iterate plus its FP32 correction).
+template <int DIM, typename R, int kLoad = 0, bool kEnergy = true, bool kAxpy = false, typename X2 = R>
 __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R* __restrict__ mom,
                                                         const uint8_t* __restrict__ bcmask,
                                                         const R* __restrict__ x, R* __restrict__ y, int i, int j,
                                                         int k, int32_t e, int c_only = -1,
-                                                        const R* __restrict__ x2 = nullptr, R beta = R(0)) {
+                                                        const X2* __restrict__ x2 = nullptr, R beta = R(0)) {
     constexpr int NS = 1 << DIM;
     constexpr int NM = n_moments<DIM>();
     const int64_t nnode = mk.nnode, nel = mk.nel;
@@ -188,10 +188,10 @@ __device__ __forceinline__ double element_apply_scatter(const MeshK& mk, const R
             m[c][2 * q] = kLoad == 1 ? __ldcg(xr) : kLoad == 2 ? __ldca(xr) : xr[0];
             m[c][2 * q + 1] = kLoad == 1 ? __ldcg(xr + 1) : kLoad == 2 ? __ldca(xr + 1) : xr[1];
             if constexpr (kAxpy) {
-                const R* pr = x2 + c * nnode + n0 + rowoff[q];
-                m[c][2 * q] = m[c][2 * q] + beta * (kLoad == 1 ? __ldcg(pr) : kLoad == 2 ? __ldca(pr) : pr[0]);
-                m[c][2 * q + 1] =
-                    m[c][2 * q + 1] + beta * (kLoad == 1 ? __ldcg(pr + 1) : kLoad == 2 ? __ldca(pr + 1) : pr[1]);
+                const X2* pr = x2 + c * nnode + n0 + rowoff[q];
+                m[c][2 * q] = m[c][2 * q] + beta * (R)(kLoad == 1 ? __ldcg(pr) : kLoad == 2 ? __ldca(pr) : pr[0]);
+                m[c][2 * q + 1] = m[c][2 * q + 1] +
+                                  beta * (R)(kLoad == 1 ? __ldcg(pr + 1) : kLoad == 2 ? __ldca(pr + 1) : pr[1]);
             }
         }
     }
@@ -218,11 +218,11 @@ struct ApplyTile<2> {
 // y += K x over the element tiles tile0, tile0 + tstride, … (blockDim.x must be 256).
 // Returns this thread's Σ x_eᵀ K_e x_e when kEnergy.
 template <int DIM, typename R, int kLoad = 0, bool kEnergy = true, int TY = ApplyTile<DIM>::Y,
-          int TZ = ApplyTile<DIM>::Z, bool kAxpy = false>
+          int TZ = ApplyTile<DIM>::Z, bool kAxpy = false, typename X2 = R>
 __device__ __forceinline__ double apply_tiles(const MeshK& mk, const R* __restrict__ mom,
                                               const uint8_t* __restrict__ bcmask, const R* __restrict__ x,
                                               R* __restrict__ y, int64_t tile0, int64_t tstride,
-                                              const R* __restrict__ x2 = nullptr, R beta = R(0)) {
+                                              const X2* __restrict__ x2 = nullptr, R beta = R(0)) {
     constexpr int TX = ApplyTile<DIM>::X;
     const int ntx = (mk.n[0] + TX - 1) / TX, nty = (mk.n[1] + TY - 1) / TY;
     const int ntz = DIM == 3 ? (mk.n[2] + TZ - 1) / TZ : 1;
@@ -233,7 +233,7 @@ __device__ __forceinline__ double apply_tiles(const MeshK& mk, const R* __restri
         const int rr = tile / ntx;
         const int i = (tile - rr * ntx) * TX + tx, j = (rr % nty) * TY + ty, k = (rr / nty) * TZ + tz;
         if (i < mk.n[0] && j < mk.n[1] && (DIM == 2 || k < mk.n[2]))
-            en += element_apply_scatter<DIM, R, kLoad, kEnergy, kAxpy>(mk, mom, bcmask, x, y, i, j, k,
+            en += element_apply_scatter<DIM, R, kLoad, kEnergy, kAxpy, X2>(mk, mom, bcmask, x, y, i, j, k,
                                                                        i + mk.n[0] * (j + mk.n[1] * k), -1, x2,
                                                                        beta);
     }
