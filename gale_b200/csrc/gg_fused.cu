@@ -859,11 +859,13 @@ constexpr int kUzBarrierFail = -1;
 // warm: start from x, whose defect b − Kx the caller has already put in r64 (else
 // x = 0).  Each phase that ends with a defect also makes the next sweep's start, so a
 // sweep costs its FCG iterations plus two phases (the FP64 apply and the defect).
+// prestarted: the caller's last phase (which ended with a grid barrier) already did the
+// first phase below (x, r64, acc64, the first sweep's start and the three partial sums).
 // Returns GG_OK / GG_ERR_NOT_CONVERGED / GG_ERR_NONFINITE, or kUzBarrierFail.
 template <int DIM>
 __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArgs& A, const double* b, double* x,
                                         double rtol, bool warm, bool& tight, unsigned int& epoch, int& its,
-                                        int& sweeps) {
+                                        int& sweeps, bool prestarted) {
     const FusedLevel& L0 = T.lv[0];
     const int64_t nnode = L0.mk.nnode;
     double* P = A.part + 4 * gridDim.x;
@@ -871,35 +873,37 @@ __device__ __forceinline__ int uz_inner(const FusedTable& T, const UzawaFusedArg
     // x = 0 and r = b on free rows (the defect of x = 0), or the warm start's defect as
     // given; acc64 = 0; the first sweep's start on r; the partials of ‖D⁻¹b‖, ‖D⁻¹r‖ and
     // the start's Σ r²
-    double acc = 0.0, acc_r = 0.0, acc32 = 0.0;
-    for (int64_t n = gtid(); n < nnode; n += gstride()) {
-        const uint8_t bm = L0.bc[n];
+    if (!prestarted) {
+        double acc = 0.0, acc_r = 0.0, acc32 = 0.0;
+        for (int64_t n = gtid(); n < nnode; n += gstride()) {
+            const uint8_t bm = L0.bc[n];
 #pragma unroll
-        for (int c = 0; c < DIM; c++) {
-            const int64_t i = (int64_t)c * nnode + n;
-            const bool fixed = (bm >> c) & 1;
-            const double bv = fixed ? 0.0 : __ldcg(&b[i]);
-            double rv = bv;
-            if (warm) rv = fixed ? 0.0 : __ldcg(&A.r64[i]);
-            if (!fixed) {
-                const double zv = bv / A.kdiag[i];
-                acc += zv * zv;
-                const double zr = rv / A.kdiag[i];
-                acc_r += zr * zr;
+            for (int c = 0; c < DIM; c++) {
+                const int64_t i = (int64_t)c * nnode + n;
+                const bool fixed = (bm >> c) & 1;
+                const double bv = fixed ? 0.0 : __ldcg(&b[i]);
+                double rv = bv;
+                if (warm) rv = fixed ? 0.0 : __ldcg(&A.r64[i]);
+                if (!fixed) {
+                    const double zv = bv / A.kdiag[i];
+                    acc += zv * zv;
+                    const double zr = rv / A.kdiag[i];
+                    acc_r += zr * zr;
+                }
+                if (!warm) {
+                    x[i] = 0.0;
+                    A.r64[i] = bv;
+                }
+                A.acc64[i] = 0.0;
+                const float r32 = (float)rv;
+                fcg_start_dof(L0, i, r32, A.e32, A.p32, A.Ap32);
+                acc32 += (double)r32 * (double)r32;
             }
-            if (!warm) {
-                x[i] = 0.0;
-                A.r64[i] = bv;
-            }
-            A.acc64[i] = 0.0;
-            const float r32 = (float)rv;
-            fcg_start_dof(L0, i, r32, A.e32, A.p32, A.Ap32);
-            acc32 += (double)r32 * (double)r32;
         }
+        put_partial2(acc, acc_r, P, P1);
+        put_partial(acc32, A.part);
+        if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
     }
-    put_partial2(acc, acc_r, P, P1);
-    put_partial(acc32, A.part);
-    if (!grid_barrier(A.gb, &epoch)) return kUzBarrierFail;
     double b2, r2;
     all_sum2(P, P1, b2, r2);
     const double rnorm0 = sqrt(b2);
@@ -978,10 +982,10 @@ __device__ __forceinline__ bool uzawa_body(const FusedTable& T, const UzawaFused
     const double* ib = A.f;  // STEP 1 (:553-565)
     double* ix = A.vstar;
     double irtol = A.tolerance;
-    bool iwarm = false;
+    bool iwarm = false, ipre = false;
     for (;;) {
         o.inner_solves++;
-        const int rc = uz_inner<DIM>(T, A, ib, ix, irtol, iwarm, tight, epoch, o.inner_iterations, o.sweeps);
+        const int rc = uz_inner<DIM>(T, A, ib, ix, irtol, iwarm, tight, epoch, o.inner_iterations, o.sweeps, ipre);
         if (rc == kUzBarrierFail) return false;
         if (rc != GG_OK) {
             o.status = rc;
@@ -1119,8 +1123,11 @@ __device__ __forceinline__ bool uzawa_body(const FusedTable& T, const UzawaFused
         // G s, and the recycled start β u*_prev of K u* = G s with its defect: the previous
         // inner solve ended with r = G s_prev − K u*_prev (its last FP64 defect, still in
         // r64, ftmp still G s_prev), so G s − K(β u*_prev) = G s − β (G s_prev − r) without
-        // an apply (free rows; 0 on Dirichlet rows)
+        // an apply (free rows; 0 on Dirichlet rows).  The same pass makes the inner solve's
+        // first phase (uz_inner, prestarted): acc64 = 0, the first sweep's start and the
+        // partial sums of ‖D⁻¹G s‖, ‖D⁻¹r‖ and the start's Σ r².
         const bool warm = A.recycle && it > 0;
+        double acc_b = 0.0, acc_r = 0.0, acc32 = 0.0;
         for (int64_t n = gtid(); n < nnode; n += gstride()) {
             double g[DIM];
             g_node<DIM, double, true>(mk, A.s, n, g);
@@ -1130,19 +1137,35 @@ __device__ __forceinline__ bool uzawa_body(const FusedTable& T, const UzawaFused
                 const int64_t i = (int64_t)c * nnode + n;
                 const bool fixed = (bm >> c) & 1;
                 const double gs = fixed ? 0.0 : g[c];
+                double rv = gs;
                 if (warm) {
                     A.vstar[i] = beta * __ldcg(&A.vstar[i]);
-                    A.r64[i] = fixed ? 0.0 : gs - beta * (__ldcg(&A.ftmp[i]) - __ldcg(&A.r64[i]));
+                    rv = fixed ? 0.0 : gs - beta * (__ldcg(&A.ftmp[i]) - __ldcg(&A.r64[i]));
+                } else {
+                    A.vstar[i] = 0.0;
                 }
+                A.r64[i] = rv;
                 A.ftmp[i] = gs;
+                A.acc64[i] = 0.0;
+                if (!fixed) {
+                    const double zb = gs / A.kdiag[i], zr = rv / A.kdiag[i];
+                    acc_b += zb * zb;
+                    acc_r += zr * zr;
+                }
+                const float r32 = (float)rv;
+                fcg_start_dof(L0, i, r32, A.e32, A.p32, A.Ap32);
+                acc32 += (double)r32 * (double)r32;
             }
         }
+        put_partial2(acc_b, acc_r, P0, P1);
+        put_partial(acc32, A.part);
         if (!grid_barrier(A.gb, &epoch)) return false;
         stage = 3;
         ib = A.ftmp;
         ix = A.vstar;
         irtol = A.inner_rtol;
         iwarm = warm;
+        ipre = true;
     }
     o.outer_iterations = it;
     o.rel_residual = exact ? 0.0 : relres;
