@@ -210,6 +210,7 @@ ABI_FUNCTIONS = {
     "gg_get_rhs": ([_P, _PD, _PD], C.c_int),
     "gg_get_diagonals": ([_P, _PD, _PD], C.c_int),
     "gg_time_apply": ([_P, C.c_int32, C.c_int32, _PD], C.c_int),
+    "gg_get_coarse_inverse": ([_P, C.POINTER(C.c_int64), C.POINTER(C.c_float), _PD], C.c_int),
     "gg_time_grid_barrier": ([C.c_int32, C.c_int32, _PD], C.c_int),
     "gg_check_grid_barrier_timeout": ([C.c_int32, C.POINTER(C.c_int32)], C.c_int),
     "gg_locate_noalloc": ([C.POINTER(MeshDesc), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -535,6 +535,15 @@ int gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_
     return GG_OK;
 }
 
+int gg_get_coarse_inverse(gg_handle* h, int64_t* n, float* inverse, double* op) {
+    if (!h || !n) return GG_ERR_INVALID;
+    Handle& H = h->H;
+    if (!H.built) return gg::err(H, GG_ERR_STATE, "operator not built");
+    int rc = GG_OK;
+    GG_TRY2(h, { rc = gg::coarse_inverse_copy(H, n, inverse, op); })
+    return rc;
+}
+
 int gg_apply_G(gg_handle* h, const double* p, double* y) {
     if (!h || !p || !y) return GG_ERR_INVALID;
     Handle& H = h->H;

@@ -79,6 +79,7 @@ ChebCoef cheb_coef(double lmax_est, int degree);
 // Chebyshev degree of level l's smoother (the configured degree on the fine level)
 int level_degree(const Handle& H, size_t l);
 int mg_setup(Handle& H);
+int coarse_inverse_copy(Handle& H, int64_t* n, float* inv, double* op);
 void vcycle(Handle& H, size_t l, const float* b, float* x, const int32_t* done);
 void mg_restrict(Handle& H, size_t l, const float* fine, float* coarse, const int32_t* done);
 void mg_prolong_add(Handle& H, size_t l, const float* coarse, float* fine, const int32_t* done);

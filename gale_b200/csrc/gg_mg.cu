@@ -502,7 +502,7 @@ static double power_lambda(Handle& H, MGLevel& L) {
 // units from shared-memory tiles); the only sequential part is the b steps inside each
 // diagonal block, n steps in all.
 constexpr int kGjB = 64;      // pivot block
-constexpr int kGjTile = 128;  // output tile of the update (256 threads × 8 × 8)
+constexpr int kGjTile = 64;   // output tile of the update (256 threads × 4 × 4)
 
 // W = A as rows (A holds the columns K e_j; K is symmetric up to the order of its FP64
 // sums, and the transpose keeps W = K exactly), BC rows and columns replaced by the identity
@@ -516,139 +516,237 @@ __global__ void k_bgj_init(int64_t n, int64_t nnode, const uint8_t* __restrict__
     }
 }
 
-// D⁻¹ of the pivot block by element-wise Gauss–Jordan steps in shared memory: one CTA of
-// 1024 threads, thread t owning entries t + 1024·r (r < 4) of the block padded to 64 × 64
-// with the identity (the padded inverse holds D⁻¹ in its top left b × b).  Each step
-// reads one copy of the block and writes the other (one barrier per step); the row
-// stride of 65 doubles keeps the pivot-column reads free of bank conflicts.
-constexpr size_t kGjPivotSmem = sizeof(double) * 2 * kGjB * (kGjB + 1);
-__global__ void __launch_bounds__(1024) k_bgj_pivot(int64_t n, int64_t k0, int b, const double* __restrict__ W,
-                                                    double* __restrict__ Dinv) {
-    extern __shared__ double s_piv[];
-    constexpr int S = kGjB + 1;
-    double* D0 = s_piv;
-    double* D1 = s_piv + kGjB * S;
-    const int t = threadIdx.x;
+// D⁻¹ of a pivot block by element-wise Gauss–Jordan steps, the block padded to 64 × 64 with
+// the identity (the padded inverse holds D⁻¹ in its top left b × b).  256 threads; thread
+// (ty, tx) keeps entries (ty + 16r, tx + 16c), r, c < 4, of the block in a[r][c] for all 64
+// steps.  A step needs, besides a thread's own entries, only the pivot row and the pivot
+// column: the threads that own row and column p + 1 publish their new values into the other
+// half of a double-buffered pair of 64-entry arrays, so each step takes one barrier.  On
+// return a[][] holds the padded inverse; the caller writes D⁻¹ out.
+__device__ __forceinline__ void gj_block_inverse(double (&a)[4][4], int ty, int tx, double (*s_row)[kGjB],
+                                                 double (*s_col)[kGjB]) {
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const int q = t + 1024 * r, i = q >> 6, j = q & 63;
-        D0[i * S + j] = (i < b && j < b) ? W[(k0 + i) * n + k0 + j] : (i == j ? 1.0 : 0.0);
-    }
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int i = ty + 16 * r, j = tx + 16 * c;
+            if (i == 0) s_row[0][j] = a[r][c];
+            if (j == 0) s_col[0][i] = a[r][c];
+        }
     __syncthreads();
     for (int p = 0; p < kGjB; p++) {
-        const double* D = (p & 1) ? D1 : D0;
-        double* E = (p & 1) ? D0 : D1;
-        const double piv = 1.0 / D[p * S + p];
+        const int h = p & 1;
+        const double piv = __drcp_rn(s_row[h][p]);
+        double dip[4], t[4];
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            const int q = t + 1024 * r, i = q >> 6, j = q & 63;
-            double v;
-            if (i == p) v = j == p ? piv : D[p * S + j] * piv;
-            else v = j == p ? -D[i * S + p] * piv : D[i * S + j] - D[i * S + p] * (D[p * S + j] * piv);
-            E[i * S + j] = v;
-        }
+        for (int r = 0; r < 4; r++) dip[r] = s_col[h][ty + 16 * r];
+#pragma unroll
+        for (int c = 0; c < 4; c++) t[c] = s_row[h][tx + 16 * c] * piv;
+        // every entry takes the elimination a − a[i][p]·(a[p][j]/a[p][p]); then the pivot
+        // row becomes a[p][j]/a[p][p] (1/a[p][p] on the diagonal) and the pivot column
+        // −a[i][p]/a[p][p]
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) a[r][c] = a[r][c] - dip[r] * t[c];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            if (ty + 16 * r == p) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) a[r][c] = tx + 16 * c == p ? piv : t[c];
+            }
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (tx + 16 * c == p) {
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+                    if (ty + 16 * r != p) a[r][c] = -dip[r] * piv;
+            }
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            if (ty + 16 * r == p + 1) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) s_row[h ^ 1][tx + 16 * c] = a[r][c];
+            }
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (tx + 16 * c == p + 1) {
+#pragma unroll
+                for (int r = 0; r < 4; r++) s_col[h ^ 1][ty + 16 * r] = a[r][c];
+            }
         __syncthreads();
     }
-    const double* D = (kGjB & 1) ? D1 : D0;  // after 64 steps the result is back in D0
+}
+
+__device__ __forceinline__ void gj_store_inverse(const double (&a)[4][4], int ty, int tx, int b,
+                                                 double* __restrict__ Dinv) {
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const int q = t + 1024 * r, i = q >> 6, j = q & 63;
-        if (i < b && j < b) Dinv[i * b + j] = D[i * S + j];
-    }
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int i = ty + 16 * r, j = tx + 16 * c;
+            if (i < b && j < b) Dinv[i * b + j] = a[r][c];
+        }
+}
+
+// D⁻¹ of the first pivot block (every later one is inverted by the update before it)
+__global__ void __launch_bounds__(256) k_bgj_pivot(int64_t n, int64_t k0, int b, const double* __restrict__ W,
+                                                   double* __restrict__ Dinv) {
+    __shared__ double s_row[2][kGjB], s_col[2][kGjB];
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    double a[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int i = ty + 16 * r, j = tx + 16 * c;
+            a[r][c] = (i < b && j < b) ? W[(k0 + i) * n + k0 + j] : (i == j ? 1.0 : 0.0);
+        }
+    gj_block_inverse(a, ty, tx, s_row, s_col);
+    gj_store_inverse(a, ty, tx, b, Dinv);
 }
 
 // The pivot block's row panel R[m][j] = (D⁻¹ W[K,:])[m][j] (columns j ∈ K: D⁻¹ itself) and
 // a copy of its column panel, stored transposed CT[m][i] = W[i][k0+m], both from W before
-// the update
-__global__ void k_bgj_panels(int64_t n, int64_t k0, int b, const double* __restrict__ W,
-                             const double* __restrict__ Dinv, double* __restrict__ R, double* __restrict__ C) {
-    const int64_t nb = (int64_t)b * n;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < 2 * nb; q += (int64_t)gridDim.x * blockDim.x) {
-        if (q < nb) {
-            const int m = (int)(q / n);
-            const int64_t j = q - (int64_t)m * n;
-            double s;
-            if (j >= k0 && j < k0 + b) {
-                s = Dinv[m * b + (j - k0)];
-            } else {
-                s = 0.0;
-                for (int l = 0; l < b; l++) s += Dinv[m * b + l] * W[(k0 + l) * n + j];
+// the update.  One CTA of 256 threads per 32 columns (blockIdx.y = 0: the row panel, D⁻¹ and the 64 × 32
+// tile of W[K,:] staged in shared memory, 8 outputs a thread, each a sum over l in order)
+// or per 32 rows (blockIdx.y = 1: the column panel, transposed through shared memory so
+// that both the reads and the writes are coalesced).
+constexpr int kGjPanelCols = 32;
+__global__ void __launch_bounds__(256) k_bgj_panels(int64_t n, int64_t k0, int b, const double* __restrict__ W,
+                                                    const double* __restrict__ Dinv, double* __restrict__ R,
+                                                    double* __restrict__ C) {
+    __shared__ double sm[kGjB * kGjB + kGjB * kGjPanelCols];  // 48 KB
+    const int64_t t0 = (int64_t)blockIdx.x * kGjPanelCols;
+    if (blockIdx.y == 0) {
+        double* Ds = sm;                // [m][l]
+        double* Ws = sm + kGjB * kGjB;  // [l][t]
+        for (int q = threadIdx.x; q < kGjB * kGjB; q += blockDim.x) {
+            const int m = q / kGjB, l = q % kGjB;
+            Ds[q] = m < b && l < b ? Dinv[m * b + l] : 0.0;
+        }
+        for (int q = threadIdx.x; q < kGjB * kGjPanelCols; q += blockDim.x) {
+            const int l = q / kGjPanelCols, t = q % kGjPanelCols;
+            Ws[q] = l < b && t0 + t < n ? W[(k0 + l) * n + t0 + t] : 0.0;
+        }
+        __syncthreads();
+        const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int m = ty + 16 * r;
+            if (m >= b) continue;
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const int64_t j = t0 + tx + 16 * c;
+                if (j >= n) continue;
+                double v;
+                if (j >= k0 && j < k0 + b) {
+                    v = Ds[m * kGjB + (j - k0)];
+                } else {
+                    v = 0.0;
+                    for (int l = 0; l < b; l++) v += Ds[m * kGjB + l] * Ws[l * kGjPanelCols + tx + 16 * c];
+                }
+                R[m * n + j] = v;
             }
-            R[m * n + j] = s;
-        } else {
-            const int64_t r = q - nb, i = r / b;
-            const int m = (int)(r - i * b);
-            C[(int64_t)m * n + i] = W[i * n + k0 + m];
+        }
+    } else {
+        constexpr int S = kGjPanelCols + 1;
+        double* Ts = sm;  // [m][i] with a row stride of 33
+        for (int q = threadIdx.x; q < kGjPanelCols * kGjB; q += blockDim.x) {
+            const int i = q / kGjB, m = q % kGjB;
+            if (m < b && t0 + i < n) Ts[m * S + i] = W[(t0 + i) * n + k0 + m];
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < kGjB * kGjPanelCols; q += blockDim.x) {
+            const int m = q / kGjPanelCols, i = q % kGjPanelCols;
+            if (m < b && t0 + i < n) C[(int64_t)m * n + t0 + i] = Ts[m * S + i];
         }
     }
 }
 
-// The rank-b update of one 128 × 128 output tile (blockIdx.x, blockIdx.y = column, row
-// tile): rows in K take the row panel, every other row W[i,j] (or 0 for j ∈ K) minus
-// C[i,:]·R[:,j].  C (stored transposed) and R tiles are staged in shared memory by
-// coalesced loads; each thread forms an 8 × 8 block of outputs (rows 4·ty + {0..3} and
-// 64 + 4·ty + {0..3}, columns likewise with tx), so a warp's shared-memory reads are
-// broadcasts or consecutive.
+// The rank-b update of one 64 × 64 output tile: rows in K take the row panel, every other
+// row W[i,j] (or 0 for j ∈ K) minus C[i,:]·R[:,j].  C (stored transposed) and R tiles are
+// staged in shared memory by coalesced loads (64 KB); each thread forms 4 × 4 outputs at a
+// stride of 16 rows and columns (a half-warp reads and writes 16 consecutive doubles), its
+// 16 old values of W loaded before the multiply-add loop so that their latency hides behind
+// it.  When a next pivot block of bn rows follows (it starts at k0 + 64, on the tile grid),
+// the CTA that updates its diagonal tile is scheduled first and goes on to invert it from
+// its registers (the layout of gj_block_inverse) into Dinv, while the others finish the
+// update: the next panels launch finds D⁻¹ ready.
 constexpr size_t kGjUpdateSmem = sizeof(double) * 2 * kGjB * kGjTile;
-__global__ void __launch_bounds__(256, 1) k_bgj_update(int64_t n, int64_t k0, int b, double* __restrict__ W,
-                                                       const double* __restrict__ R, const double* __restrict__ C) {
+__global__ void __launch_bounds__(256) k_bgj_update(int64_t n, int64_t k0, int b, double* __restrict__ W,
+                                                    const double* __restrict__ R, const double* __restrict__ C,
+                                                    int bn, double* __restrict__ Dinv) {
     extern __shared__ double s_bgj[];
+    __shared__ double s_row[2][kGjB], s_col[2][kGjB];
     double* Cs = s_bgj;                   // [kGjB][kGjTile]
     double* Rs = s_bgj + kGjB * kGjTile;  // [kGjB][kGjTile]
-    const int64_t i0 = (int64_t)blockIdx.y * kGjTile, j0 = (int64_t)blockIdx.x * kGjTile;
+    const int64_t nt = (n + kGjTile - 1) / kGjTile;
+    const int64_t dn = bn > 0 ? ((k0 + kGjB) / kGjTile) * (nt + 1) : 0;  // the next diagonal tile
+    int64_t tile = blockIdx.x;
+    if (tile == 0) tile = dn;
+    else if (tile == dn) tile = 0;
+    const int64_t i0 = (tile / nt) * kGjTile, j0 = (tile % nt) * kGjTile;
     for (int q = threadIdx.x; q < kGjB * kGjTile; q += blockDim.x) {
         const int m = q / kGjTile, t = q % kGjTile;
         const bool ok = m < b;
         Cs[q] = ok && i0 + t < n ? C[(int64_t)m * n + i0 + t] : 0.0;
         Rs[q] = ok && j0 + t < n ? R[(int64_t)m * n + j0 + t] : 0.0;
     }
-    __syncthreads();
     const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-    double acc[8][8];
+    double old[4][4];
 #pragma unroll
-    for (int r = 0; r < 8; r++)
+    for (int r = 0; r < 4; r++) {
+        const int64_t i = i0 + ty + 16 * r;
 #pragma unroll
-        for (int c = 0; c < 8; c++) acc[r][c] = 0.0;
-    for (int m = 0; m < b; m++) {
-        const double* cm = Cs + m * kGjTile;
-        const double* rm = Rs + m * kGjTile;
-        double cv[8], rv[8];
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const double2 c01 = *reinterpret_cast<const double2*>(cm + 64 * h + 4 * ty);
-            const double2 c23 = *reinterpret_cast<const double2*>(cm + 64 * h + 4 * ty + 2);
-            const double2 r01 = *reinterpret_cast<const double2*>(rm + 64 * h + 4 * tx);
-            const double2 r23 = *reinterpret_cast<const double2*>(rm + 64 * h + 4 * tx + 2);
-            cv[4 * h] = c01.x;
-            cv[4 * h + 1] = c01.y;
-            cv[4 * h + 2] = c23.x;
-            cv[4 * h + 3] = c23.y;
-            rv[4 * h] = r01.x;
-            rv[4 * h + 1] = r01.y;
-            rv[4 * h + 2] = r23.x;
-            rv[4 * h + 3] = r23.y;
+        for (int c = 0; c < 4; c++) {
+            const int64_t j = j0 + tx + 16 * c;
+            const bool keep = i < n && j < n && !(i >= k0 && i < k0 + b) && !(j >= k0 && j < k0 + b);
+            old[r][c] = keep ? W[i * n + j] : 0.0;
         }
+    }
+    __syncthreads();
+    double acc[4][4];
 #pragma unroll
-        for (int r = 0; r < 8; r++)
+    for (int r = 0; r < 4; r++)
 #pragma unroll
-            for (int c = 0; c < 8; c++) acc[r][c] += cv[r] * rv[c];
+        for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
+    for (int m = 0; m < b; m++) {
+        double cv[4], rv[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) cv[r] = Cs[m * kGjTile + ty + 16 * r];
+#pragma unroll
+        for (int c = 0; c < 4; c++) rv[c] = Rs[m * kGjTile + tx + 16 * c];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[r][c] += cv[r] * rv[c];
     }
 #pragma unroll
-    for (int r = 0; r < 8; r++) {
-        const int64_t i = i0 + 64 * (r >> 2) + 4 * ty + (r & 3);
+    for (int r = 0; r < 4; r++) {
+        const int64_t i = i0 + ty + 16 * r;
         if (i >= n) continue;
         const bool rowK = i >= k0 && i < k0 + b;
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const int64_t j = j0 + 64 * (c >> 2) + 4 * tx + (c & 3);
+        for (int c = 0; c < 4; c++) {
+            const int64_t j = j0 + tx + 16 * c;
             if (j >= n) continue;
-            if (rowK) {
-                W[i * n + j] = R[(i - k0) * n + j];
-            } else {
-                const double base = (j >= k0 && j < k0 + b) ? 0.0 : W[i * n + j];
-                W[i * n + j] = base - acc[r][c];
-            }
+            const double v = rowK ? R[(i - k0) * n + j] : old[r][c] - acc[r][c];
+            W[i * n + j] = v;
+            acc[r][c] = v;
         }
+    }
+    if (bn > 0 && tile == dn) {
+        // this tile is the next pivot block: rows and columns k0 + 64 + [0, bn)
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int i = ty + 16 * r, j = tx + 16 * c;
+                if (!(i < bn && j < bn)) acc[r][c] = i == j ? 1.0 : 0.0;
+            }
+        gj_block_inverse(acc, ty, tx, s_row, s_col);
+        gj_store_inverse(acc, ty, tx, bn, Dinv);
     }
 }
 
@@ -702,8 +800,9 @@ __global__ void k_coarse_columns(MeshK mk, const double* __restrict__ mom, const
 
 // Dense FP32 inverse of the coarsest operator: its columns by unit-vector applies (FP64),
 // then the blocked Gauss–Jordan inversion above (FP64), rounded to FP32 with rows padded
-// to a multiple of 4.  3 launches per pivot block of 64: C2's 8³ level (2,187 dofs) takes
-// 35 blocks.
+// to a multiple of 4.  Two launches per pivot block of 64 (panels, update with the next
+// block's inverse) after one for the first block's inverse: the 8³ level of a 64³ mesh
+// (2,187 dofs) takes 35 blocks.
 static void coarse_inverse(Handle& H, MGLevel& L) {
     const int64_t n = L.ndof;
     const int64_t ld = (n + 3) & ~(int64_t)3;
@@ -724,17 +823,19 @@ static void coarse_inverse(Handle& H, MGLevel& L) {
     GG_CUDA(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && !smem_set[dev].load()) {
         GG_CUDA(cudaFuncSetAttribute(k_bgj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjUpdateSmem));
-        GG_CUDA(cudaFuncSetAttribute(k_bgj_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjPivotSmem));
         smem_set[dev].store(true);
     }
-    const dim3 tiles((unsigned)((n + kGjTile - 1) / kGjTile), (unsigned)((n + kGjTile - 1) / kGjTile));
+    const unsigned tiles = (unsigned)(((n + kGjTile - 1) / kGjTile) * ((n + kGjTile - 1) / kGjTile));
+    const dim3 panels((unsigned)((n + kGjPanelCols - 1) / kGjPanelCols), 2);
     int64_t launches = 0;
+    k_bgj_pivot<<<1, 256, 0, st>>>(n, 0, (int)std::min<int64_t>(kGjB, n), W, Dinv);
+    launches++;
     for (int64_t k0 = 0; k0 < n; k0 += kGjB) {
         const int b = (int)std::min<int64_t>(kGjB, n - k0);
-        k_bgj_pivot<<<1, 1024, kGjPivotSmem, st>>>(n, k0, b, W, Dinv);
-        k_bgj_panels<<<grid_for(2 * (int64_t)b * n, 256), 256, 0, st>>>(n, k0, b, W, Dinv, R, Cp);
-        k_bgj_update<<<tiles, 256, kGjUpdateSmem, st>>>(n, k0, b, W, R, Cp);
-        launches += 3;
+        const int bn = (int)std::max<int64_t>(0, std::min<int64_t>(kGjB, n - k0 - kGjB));
+        k_bgj_panels<<<panels, 256, 0, st>>>(n, k0, b, W, Dinv, R, Cp);
+        k_bgj_update<<<tiles, 256, kGjUpdateSmem, st>>>(n, k0, b, W, R, Cp, bn, Dinv);
+        launches += 2;
     }
     H.coarse_inv.ensure(sizeof(float) * n * ld);
     k_bgj_extract<<<grid_for(n * ld, 256), 256, 0, st>>>(n, ld, W, H.coarse_inv.as<float>());
@@ -746,6 +847,30 @@ static void coarse_inverse(Handle& H, MGLevel& L) {
 }
 
 // Build (or refresh for a new operator) the hierarchy.  Needs the mixed build (FP32 moments).
+// Copies of the coarsest level's dense FP32 inverse (rows of n) and of the FP64 operator it
+// inverts (row-major, Dirichlet rows and columns replaced by the identity), for inspection.
+int coarse_inverse_copy(Handle& H, int64_t* n, float* inv, double* op) {
+    const int rc = mg_setup(H);
+    if (rc != GG_OK) return rc;
+    *n = H.coarse_n;
+    if (!H.coarse_n) return GG_OK;
+    const int64_t m = H.coarse_n;
+    cudaStream_t st = H.stream;
+    if (inv)
+        GG_CUDA(cudaMemcpy2DAsync(inv, sizeof(float) * m, H.coarse_inv.p, sizeof(float) * H.coarse_ld,
+                                  sizeof(float) * m, m, cudaMemcpyDeviceToHost, st));
+    if (op) {
+        MGLevel& L = *H.mg.back();
+        double* A = H.mg_dense.as<double>();  // the operator's columns, kept after the inversion
+        double* W = A + m * m;
+        k_bgj_init<<<grid_for(m * m, 256), 256, 0, st>>>(m, L.nnode, L.bcmask, A, W);
+        GG_CUDA(cudaGetLastError());
+        GG_CUDA(cudaMemcpyAsync(op, W, sizeof(double) * m * m, cudaMemcpyDeviceToHost, st));
+    }
+    GG_CUDA(cudaStreamSynchronize(st));
+    return GG_OK;
+}
+
 int mg_setup(Handle& H) {
     if (H.mg_gen == H.build_gen && !H.mg.empty()) return GG_OK;
     cudaStream_t st = H.stream;

@@ -429,6 +429,14 @@ GG_API int  gg_learned_eval(gg_handle* h, int32_t level, int32_t batch, const fl
  * K apply over `reps` back-to-back launches on the handle's stream, CUDA events.       */
 GG_API int  gg_time_apply(gg_handle* h, int32_t precision, int32_t reps, double* ms_per_launch);
 
+/* Inspection only (no reference counterpart): the multigrid hierarchy's dense coarse
+ * solve.  Sets up the hierarchy of the built operator if needed and returns in *n the
+ * size of its coarsest level (0: that level has no dense inverse); when the pointers are
+ * non-null, fills inverse[n*n] with the FP32 inverse the solver applies and op[n*n] with
+ * the FP64 operator it inverts, both row-major, the Dirichlet rows and columns of the
+ * operator replaced by the identity.                                                    */
+GG_API int  gg_get_coarse_inverse(gg_handle* h, int64_t* n, float* inverse, double* op);
+
 /* Measurement only (no reference counterpart): microseconds per grid barrier of the
  * persistent kernels, `iters` barriers in one cooperative launch of `blocks_per_sm`
  * blocks of 256 threads per SM on the current device (CUDA events, default stream).   */
