@@ -669,10 +669,15 @@ __global__ void __launch_bounds__(256) k_bgj_panels(int64_t n, int64_t k0, int b
 // staged in shared memory by coalesced loads (64 KB); each thread forms 4 × 4 outputs at a
 // stride of 16 rows and columns (a half-warp reads and writes 16 consecutive doubles), its
 // 16 old values of W loaded before the multiply-add loop so that their latency hides behind
-// it.  When a next pivot block of bn rows follows (it starts at k0 + 64, on the tile grid),
-// the CTA that updates its diagonal tile is scheduled first and goes on to invert it from
-// its registers (the layout of gj_block_inverse) into Dinv, while the others finish the
-// update: the next panels launch finds D⁻¹ ready.
+// it.  The in-place inverse of a symmetric matrix keeps a fixed structure: with P the
+// blocks already eliminated and U the rest, W[P,P] and W[U,U] are symmetric and
+// W[U,P] = −W[P,U]ᵀ.  So one CTA per tile (I, J) with I ≤ J (tiles are the pivot blocks)
+// computes its tile and, for I < J, writes the mirror tile (J, I), transposed through
+// shared memory with the sign −1 when exactly one of I, J is in P after this step.  That
+// halves the multiply-adds.  When a next pivot block of bn rows follows (it starts at
+// k0 + 64, on the tile grid), the CTA that updates its diagonal tile is scheduled first and
+// goes on to invert it from its registers (the layout of gj_block_inverse) into Dinv, while
+// the others finish the update: the next panels launch finds D⁻¹ ready.
 constexpr size_t kGjUpdateSmem = sizeof(double) * 2 * kGjB * kGjTile;
 __global__ void __launch_bounds__(256) k_bgj_update(int64_t n, int64_t k0, int b, double* __restrict__ W,
                                                     const double* __restrict__ R, const double* __restrict__ C,
@@ -682,11 +687,17 @@ __global__ void __launch_bounds__(256) k_bgj_update(int64_t n, int64_t k0, int b
     double* Cs = s_bgj;                   // [kGjB][kGjTile]
     double* Rs = s_bgj + kGjB * kGjTile;  // [kGjB][kGjTile]
     const int64_t nt = (n + kGjTile - 1) / kGjTile;
-    const int64_t dn = bn > 0 ? ((k0 + kGjB) / kGjTile) * (nt + 1) : 0;  // the next diagonal tile
+    const int64_t kb = k0 / kGjTile;  // this step's pivot block
+    // upper-triangle tile t ↔ (I, J), I ≤ J: row I starts at off(I) = I·nt − I(I−1)/2
+    auto off = [nt](int64_t I) { return I * nt - I * (I - 1) / 2; };
+    const int64_t dn = bn > 0 ? off(kb + 1) : 0;  // the next diagonal tile (kb + 1, kb + 1)
     int64_t tile = blockIdx.x;
     if (tile == 0) tile = dn;
     else if (tile == dn) tile = 0;
-    const int64_t i0 = (tile / nt) * kGjTile, j0 = (tile % nt) * kGjTile;
+    int64_t I = 0;
+    while (off(I + 1) <= tile) I++;
+    const int64_t J = I + (tile - off(I));
+    const int64_t i0 = I * kGjTile, j0 = J * kGjTile;
     for (int q = threadIdx.x; q < kGjB * kGjTile; q += blockDim.x) {
         const int m = q / kGjTile, t = q % kGjTile;
         const bool ok = m < b;
@@ -734,6 +745,22 @@ __global__ void __launch_bounds__(256) k_bgj_update(int64_t n, int64_t k0, int b
             const double v = rowK ? R[(i - k0) * n + j] : old[r][c] - acc[r][c];
             W[i * n + j] = v;
             acc[r][c] = v;
+        }
+    }
+    if (I != J) {
+        constexpr int S = kGjTile + 1;
+        const double sgn = ((I <= kb) != (J <= kb)) ? -1.0 : 1.0;
+        double* Ts = s_bgj;  // [j - j0][i - i0]
+        __syncthreads();     // every thread is done with the C and R tiles
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) Ts[(tx + 16 * c) * S + ty + 16 * r] = sgn * acc[r][c];
+        __syncthreads();
+        for (int q = threadIdx.x; q < kGjTile * kGjTile; q += blockDim.x) {
+            const int jl = q / kGjTile, il = q % kGjTile;
+            const int64_t j = j0 + jl, i = i0 + il;
+            if (i < n && j < n) W[j * n + i] = Ts[jl * S + il];
         }
     }
     if (bn > 0 && tile == dn) {
@@ -825,7 +852,8 @@ static void coarse_inverse(Handle& H, MGLevel& L) {
         GG_CUDA(cudaFuncSetAttribute(k_bgj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjUpdateSmem));
         smem_set[dev].store(true);
     }
-    const unsigned tiles = (unsigned)(((n + kGjTile - 1) / kGjTile) * ((n + kGjTile - 1) / kGjTile));
+    const int64_t ntile = (n + kGjTile - 1) / kGjTile;
+    const unsigned tiles = (unsigned)(ntile * (ntile + 1) / 2);  // I ≤ J
     const dim3 panels((unsigned)((n + kGjPanelCols - 1) / kGjPanelCols), 2);
     int64_t launches = 0;
     k_bgj_pivot<<<1, 256, 0, st>>>(n, 0, (int)std::min<int64_t>(kGjB, n), W, Dinv);
