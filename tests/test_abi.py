@@ -63,3 +63,14 @@ def test_create_without_device_or_invalid_mesh():
         from gale_b200.stokes import Mesh
         m = Mesh(2, (4, 4))
         assert lib.gg_create(C.byref(m), C.byref(h)) == abi.GG_ERR_NO_DEVICE
+
+
+def test_inspection_entries_refuse_null_handles():
+    # argument checks come before any device call
+    if not os.path.exists(abi.LIB_PATH):
+        pytest.skip("library not built")
+    lib = abi.load_library()
+    n = C.c_int64(-1)
+    assert lib.gg_get_coarse_inverse(None, C.byref(n), None, None) == abi.GG_ERR_INVALID
+    assert lib.gg_get_coarse_inverse(C.c_void_p(1), None, None, None) == abi.GG_ERR_INVALID
+    assert n.value == -1
