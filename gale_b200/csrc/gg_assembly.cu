@@ -23,6 +23,8 @@
 // of the K diagonal and of the force go to per-element buffers; k_gather_corners sums
 // them per node in a fixed element order, so a build gives the same bits on every run.
 #include <map>
+#include <set>
+#include <condition_variable>
 #include <mutex>
 #include <tuple>
 
@@ -486,11 +488,15 @@ static void launch_build_shape(int shape, Handle& H, int prev, const double* pu,
 }
 
 // Autotuner: the first build of a (device, dim, precision, points-per-element class) times
-// every CTA shape once on the real inputs (each trial overwrites every output) and keeps
-// the fastest for the rest of the process.
+// every CTA shape twice on the real inputs (each trial overwrites every output) and keeps
+// the fastest for the rest of the process.  One thread tunes a key while the builds of
+// other threads with the same key wait for its choice: concurrent tunings would time each
+// other's launches and pick a shape at random.
 struct BuildTuner {
     std::mutex mu;
+    std::condition_variable cv;
     std::map<std::tuple<int, int, int, int>, int> best;
+    std::set<std::tuple<int, int, int, int>> busy;
 };
 static BuildTuner& tuner() {
     static BuildTuner t;
@@ -506,29 +512,55 @@ static void launch_build(Handle& H, int prev, const double* pu, const double* pp
     const int klass = ppe < 12 ? 0 : ppe < 24 ? 1 : ppe < 48 ? 2 : 3;
     const auto key = std::make_tuple(dev, DIM, (int)sizeof(R), klass);
     int shape = -1;
+    bool tune = false;
     {
-        std::lock_guard<std::mutex> lk(tuner().mu);
-        auto it = tuner().best.find(key);
-        if (it != tuner().best.end()) shape = it->second;
+        std::unique_lock<std::mutex> lk(tuner().mu);
+        for (;;) {
+            auto it = tuner().best.find(key);
+            if (it != tuner().best.end()) {
+                shape = it->second;
+                break;
+            }
+            if (!tuner().busy.count(key)) {
+                tuner().busy.insert(key);
+                tune = true;
+                break;
+            }
+            tuner().cv.wait(lk);
+        }
     }
-    if (shape < 0) {
+    if (tune) {
         float best_ms = 1e30f;
         int best = 2;
-        for (int k = 0; k < kNumShapes; k++) {
-            GG_CUDA(cudaEventRecord(H.ev0, H.stream));
-            launch_build_shape<DIM, R>(k, H, prev, pu, pp, mom, kdiag, sdiag, f, outputs);
-            GG_CUDA(cudaEventRecord(H.ev1, H.stream));
-            GG_CUDA(cudaEventSynchronize(H.ev1));
-            float ms = 0.f;
-            GG_CUDA(cudaEventElapsedTime(&ms, H.ev0, H.ev1));
-            if (ms < best_ms) {
-                best_ms = ms;
-                best = k;
+        try {
+            for (int rep = 0; rep < 2; rep++)
+                for (int k = 0; k < kNumShapes; k++) {
+                    GG_CUDA(cudaEventRecord(H.ev0, H.stream));
+                    launch_build_shape<DIM, R>(k, H, prev, pu, pp, mom, kdiag, sdiag, f, outputs);
+                    GG_CUDA(cudaEventRecord(H.ev1, H.stream));
+                    GG_CUDA(cudaEventSynchronize(H.ev1));
+                    float ms = 0.f;
+                    GG_CUDA(cudaEventElapsedTime(&ms, H.ev0, H.ev1));
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = k;
+                    }
+                }
+        } catch (...) {
+            {
+                std::lock_guard<std::mutex> lk(tuner().mu);
+                tuner().busy.erase(key);
             }
+            tuner().cv.notify_all();
+            throw;
         }
         shape = best;
-        std::lock_guard<std::mutex> lk(tuner().mu);
-        tuner().best[key] = shape;
+        {
+            std::lock_guard<std::mutex> lk(tuner().mu);
+            tuner().best[key] = shape;
+            tuner().busy.erase(key);
+        }
+        tuner().cv.notify_all();
     }
     H.build_shape[sizeof(R) == 4 ? 1 : 0] = shape;
     launch_build_shape<DIM, R>(shape, H, prev, pu, pp, mom, kdiag, sdiag, f, outputs);
